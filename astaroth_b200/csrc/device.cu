@@ -1,0 +1,1364 @@
+// Device layer of the B200 MHD solver: the acDevice* entry points of
+// include/astaroth.h (reference src/core/device.cc:23-538 and
+// src/core/kernels/kernels.cu:102-251) over the kernels in solve.cuh, halo.cuh
+// and reduce.cuh, plus the additions declared in include/astaroth_b200.h.
+//
+// Differences of design from the reference, all invisible at the interface:
+//   - the eight fields of `in` (and of `out`) live in one allocation with a
+//     padded row pitch (common.cuh: Layout); load/store translate between the
+//     caller's flat mx*my*mz arrays and that layout with pitched copies;
+//   - the run-time parameters ("uniforms") are a per-Device host mirror of
+//     AcMeshInfo, turned into pre-scaled kernel arguments at each launch,
+//     instead of one __constant__ AcMeshInfo per GPU; loads keep the
+//     reference's rule of skipping NaN/inf values with a warning;
+//   - reductions use per-device FP64 scratch of one double per CTA.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+
+#include "astaroth.h"
+#include "astaroth_b200.h"
+#include "common.cuh"
+#include "halo.cuh"
+#include "reduce.cuh"
+#include "solve.cuh"
+
+// ---------------------------------------------------------------------------
+// Solve configurations (tile width, tile height, ring depth)
+// ---------------------------------------------------------------------------
+#if AC_DOUBLE_PRECISION == 1
+using SolveCfg0 = TileCfg<32, 4, 8, 1>;
+using SolveCfg1 = TileCfg<16, 8, 8, 1>;
+using SolveCfg2 = TileCfg<32, 2, 10, 2>;
+#else
+using SolveCfg0 = TileCfg<32, 8, 9, 1>;
+using SolveCfg1 = TileCfg<32, 4, 10, 1>;
+using SolveCfg2 = TileCfg<64, 4, 8, 1>;
+#endif
+
+typedef void (*SolveKernelFn)(const CUtensorMap, const SolveArgs<AcReal>);
+
+struct SolveConfig {
+    const char* name;
+    int TX, TY, NP, threads;
+    size_t smem;
+    SolveKernelFn kern[3];
+};
+
+template <class Cfg>
+static SolveConfig
+make_config(const char* name)
+{
+    SolveConfig c;
+    c.name    = name;
+    c.TX      = Cfg::TX;
+    c.TY      = Cfg::TY;
+    c.NP      = Cfg::NP;
+    c.threads = Cfg::THREADS;
+    c.smem    = Cfg::smem_bytes();
+    c.kern[0] = solve_kernel<Cfg, 0>;
+    c.kern[1] = solve_kernel<Cfg, 1>;
+    c.kern[2] = solve_kernel<Cfg, 2>;
+    return c;
+}
+
+static const SolveConfig*
+solve_configs(int* n)
+{
+#if AC_DOUBLE_PRECISION == 1
+    static const SolveConfig table[] = {
+        make_config<SolveCfg0>("tile32x4_ring8"),
+        make_config<SolveCfg1>("tile16x8_ring8"),
+        make_config<SolveCfg2>("tile32x2_ring10"),
+    };
+#else
+    static const SolveConfig table[] = {
+        make_config<SolveCfg0>("tile32x8_ring9"),
+        make_config<SolveCfg1>("tile32x4_ring10"),
+        make_config<SolveCfg2>("tile64x4_ring8"),
+    };
+#endif
+    *n = (int)(sizeof(table) / sizeof(table[0]));
+    return table;
+}
+
+static const int kDefaultSolveConfig = 0;
+
+// ---------------------------------------------------------------------------
+// The device object
+// ---------------------------------------------------------------------------
+struct device_s {
+    int id;
+    AcMeshInfo local_config;
+    AcMeshInfo uniforms; // host mirror of the device parameters
+    cudaStream_t streams[NUM_STREAMS];
+    int num_sms;
+
+    Layout L;
+    state_t* blk[2]; // the two field blocks; blk[cur] is `in`
+    float* lo[2];    // mixed build: lo parts of the blocks
+    int cur;
+
+    CUtensorMap tmap[2];
+    int tmap_cfg; // configuration the maps were encoded for (-1: none)
+
+    double* red_partials;
+    int red_max_blocks;
+    unsigned* red_counter;
+    double* red_result;
+    double* h_result; // pinned
+
+    double* xfer; // device staging buffer for the double-precision views
+    size_t xfer_elems;
+
+    unsigned* status;
+    int solve_cfg;
+    int forcing;
+    unsigned long long launches;
+    unsigned long long uniform_version;
+
+    // whole-step graphs, one per starting buffer parity
+    cudaGraphExec_t graph[2];
+    unsigned long long graph_key[2];
+};
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+static inline bool
+real_is_valid(double v)
+{
+    return !isnan(v) && !isinf(v);
+}
+
+static inline cudaStream_t
+stream_of(const Device d, Stream s)
+{
+    if (s < 0 || s >= NUM_STREAMS)
+        s = STREAM_DEFAULT;
+    return d->streams[s];
+}
+
+typedef CUresult (*PFN_encodeTiled_t)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                      const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                      const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                      CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiled_t
+get_encode_tiled()
+{
+    static PFN_encodeTiled_t fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_encodeTiled_t)p;
+    }
+    return fn;
+}
+
+// 4-D map (x, y, z, field) over one field block with a (TX+8, TY+6, 1, 8) box
+static AcResult
+encode_block_map(const Device d, int b, const SolveConfig& cfg, CUtensorMap* map)
+{
+    PFN_encodeTiled_t enc = get_encode_tiled();
+    if (!enc) {
+        fprintf(stderr, "astaroth_b200: cuTensorMapEncodeTiled unavailable\n");
+        return AC_FAILURE;
+    }
+    const Layout& L          = d->L;
+    const cuuint64_t esz     = sizeof(state_t);
+    const cuuint64_t dim[4]  = {(cuuint64_t)L.mxp, (cuuint64_t)L.my, (cuuint64_t)L.mz, ACB_NF};
+    const cuuint64_t str[3]  = {(cuuint64_t)L.mxp * esz, (cuuint64_t)L.plane * esz,
+                               (cuuint64_t)L.fstride * esz};
+    const cuuint32_t box[4]  = {(cuuint32_t)(cfg.TX + 8), (cuuint32_t)(cfg.TY + 2 * NGHOST), 1,
+                               ACB_NF};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUtensorMapDataType dt = sizeof(state_t) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                                        : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    CUresult r = enc(map, dt, 4, (void*)d->blk[b], dim, str, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        fprintf(stderr, "astaroth_b200: cuTensorMapEncodeTiled failed (%d)\n", (int)r);
+        return AC_FAILURE;
+    }
+    return AC_SUCCESS;
+}
+
+static AcResult
+ensure_maps(const Device d)
+{
+    if (d->tmap_cfg == d->solve_cfg)
+        return AC_SUCCESS;
+    int n;
+    const SolveConfig* cfgs = solve_configs(&n);
+    for (int b = 0; b < 2; ++b)
+        if (encode_block_map(d, b, cfgs[d->solve_cfg], &d->tmap[b]) != AC_SUCCESS)
+            return AC_FAILURE;
+    d->tmap_cfg = d->solve_cfg;
+    return AC_SUCCESS;
+}
+
+static AcResult
+prepare_kernels_once()
+{
+    static bool done = false;
+    if (done)
+        return AC_SUCCESS;
+    int n;
+    const SolveConfig* cfgs = solve_configs(&n);
+    for (int c = 0; c < n; ++c)
+        for (int s = 0; s < 3; ++s)
+            ACB_CUDA_CHECK(cudaFuncSetAttribute((const void*)cfgs[c].kern[s],
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)cfgs[c].smem));
+    done = true;
+    return AC_SUCCESS;
+}
+
+// Kernel arguments from the uniform mirror (coefficients pre-scaled in double,
+// rounded once to AcReal).
+static SolveParams<AcReal>
+make_params(const Device d, int step)
+{
+    const AcReal* rp = d->uniforms.real_params;
+    SolveParams<AcReal> P;
+    memset(&P, 0, sizeof(P));
+    const double inv[3] = {rp[AC_inv_dsx], rp[AC_inv_dsy], rp[AC_inv_dsz]};
+    const double c1[3]  = {3.0 / 4.0, -3.0 / 20.0, 1.0 / 60.0};
+    const double c2[4]  = {-49.0 / 18.0, 3.0 / 2.0, -3.0 / 20.0, 1.0 / 90.0};
+    const double cx[3]  = {270.0 / 720.0, -27.0 / 720.0, 2.0 / 720.0};
+    for (int a = 0; a < 3; ++a) {
+        for (int k = 0; k < 3; ++k)
+            P.c1[a][k] = (AcReal)(c1[k] * inv[a]);
+        for (int k = 0; k < 4; ++k)
+            P.c2[a][k] = (AcReal)(c2[k] * inv[a] * inv[a]);
+    }
+    const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2}; // xy, xz, yz
+    for (int p = 0; p < 3; ++p)
+        for (int k = 0; k < 3; ++k)
+            P.cx[p][k] = (AcReal)(cx[k] * inv[pa[p]] * inv[pb[p]]);
+
+    const double gamma = rp[AC_gamma], cp = rp[AC_cp_sound], mu0 = rp[AC_mu0];
+    P.nu           = rp[AC_nu_visc];
+    P.eta          = rp[AC_eta];
+    P.inv_mu0      = (AcReal)(1.0 / mu0);
+    P.eta_mu0      = (AcReal)((double)rp[AC_eta] * mu0);
+    P.zeta         = rp[AC_zeta];
+    P.cs2_sound    = rp[AC_cs2_sound];
+    P.inv_cp       = (AcReal)(1.0 / cp);
+    P.gamma        = (AcReal)gamma;
+    P.gm1          = (AcReal)(gamma - 1.0);
+    P.gamma_inv_cp = (AcReal)(gamma / cp);
+    P.lnrho0       = rp[AC_lnrho0];
+    P.lnT0         = rp[AC_lnT0];
+    P.k_heat       = (AcReal)0.001; // AC_THERMAL_CONDUCTIVITY of the module
+
+    // Williamson (1980) 2N coefficients, "previous state" form
+    const double alpha[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+    const double beta[3]  = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+    const double dt       = rp[AC_dt];
+    P.rkB                 = (AcReal)(beta[step] * dt);
+    P.rkA                 = step > 0 ? (AcReal)(beta[step] * alpha[step] / beta[step - 1]) : 0;
+
+    P.forcing = d->forcing;
+    if (d->forcing) {
+        const double cs    = sqrt((double)rp[AC_cs2_sound]);
+        const double kaver = rp[AC_kaver];
+        const double NN    = cs * (double)rp[AC_forcing_magnitude] * sqrt(kaver * cs);
+        P.fscale           = (AcReal)(sqrt(dt) * NN);
+        P.fk[0]            = rp[AC_k_forcex];
+        P.fk[1]            = rp[AC_k_forcey];
+        P.fk[2]            = rp[AC_k_forcez];
+        P.ff_re[0]         = rp[AC_ff_hel_rex];
+        P.ff_re[1]         = rp[AC_ff_hel_rey];
+        P.ff_re[2]         = rp[AC_ff_hel_rez];
+        P.ff_im[0]         = rp[AC_ff_hel_imx];
+        P.ff_im[1]         = rp[AC_ff_hel_imy];
+        P.ff_im[2]         = rp[AC_ff_hel_imz];
+        P.fcphi            = (AcReal)cos((double)rp[AC_forcing_phase]);
+        P.fsphi            = (AcReal)sin((double)rp[AC_forcing_phase]);
+        const int3 gn      = d->uniforms.int3_params[AC_global_grid_n];
+        const int nn[3]    = {gn.x > 0 ? gn.x : d->L.nx, gn.y > 0 ? gn.y : d->L.ny,
+                           gn.z > 0 ? gn.z : d->L.nz};
+        const double ds[3] = {rp[AC_dsx], rp[AC_dsy], rp[AC_dsz]};
+        for (int c = 0; c < 3; ++c) {
+            P.fds[c] = (AcReal)ds[c];
+            P.fxs[c] = (AcReal)(2.0 * M_PI / (ds[c] * nn[c]));
+        }
+    }
+    return P;
+}
+
+static bool
+box_in_interior(const Device d, int3 s, int3 e)
+{
+    const Layout& L = d->L;
+    return s.x >= NGHOST && s.y >= NGHOST && s.z >= NGHOST && e.x <= NGHOST + L.nx &&
+           e.y <= NGHOST + L.ny && e.z <= NGHOST + L.nz;
+}
+
+static AcResult
+launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e)
+{
+    if (step < 0 || step > 2) {
+        fprintf(stderr, "astaroth_b200: invalid substep %d\n", step);
+        return AC_FAILURE;
+    }
+    if (!box_in_interior(d, s, e)) {
+        fprintf(stderr, "astaroth_b200: integration box outside the computational domain\n");
+        return AC_FAILURE;
+    }
+    if (e.x <= s.x || e.y <= s.y || e.z <= s.z)
+        return AC_SUCCESS;
+    if (prepare_kernels_once() != AC_SUCCESS || ensure_maps(d) != AC_SUCCESS)
+        return AC_FAILURE;
+    int n;
+    const SolveConfig& cfg = solve_configs(&n)[d->solve_cfg];
+
+    SolveArgs<AcReal> a;
+    memset(&a, 0, sizeof(a));
+    SolveGeom& g = a.g;
+    g.L          = d->L;
+    g.start      = s;
+    g.end        = e;
+    g.tx0        = (s.x - NGHOST) / cfg.TX;
+    g.ntx        = (e.x - 1 - NGHOST) / cfg.TX - g.tx0 + 1;
+    g.nty        = (e.y - s.y + cfg.TY - 1) / cfg.TY;
+    g.nzr        = e.z - s.z;
+    g.units      = (long long)g.ntx * g.nty * g.nzr;
+    a.out        = d->blk[d->cur ^ 1];
+    a.in_lo      = d->lo[d->cur];
+    a.out_lo     = d->lo[d->cur ^ 1];
+    a.status     = d->status;
+    a.P          = make_params(d, step);
+
+    int per_sm = 0;
+    ACB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.kern[step],
+                                                                 cfg.threads, cfg.smem));
+    if (per_sm < 1)
+        per_sm = 1;
+    long long grid = (long long)d->num_sms * per_sm;
+    if (grid > g.units)
+        grid = g.units;
+    cfg.kern[step]<<<(unsigned)grid, cfg.threads, cfg.smem, st>>>(d->tmap[d->cur], a);
+    ACB_CUDA_CHECK(cudaGetLastError());
+    d->launches++;
+    return AC_SUCCESS;
+}
+
+static AcResult
+launch_halo(const Device d, cudaStream_t st, int3 s, int3 e, int f0, int f1)
+{
+    const Layout& L = d->L;
+    s.x             = std::max(s.x, 0);
+    s.y             = std::max(s.y, 0);
+    s.z             = std::max(s.z, 0);
+    e.x             = std::min(e.x, L.mx);
+    e.y             = std::min(e.y, L.my);
+    e.z             = std::min(e.z, L.mz);
+    if (e.x <= s.x || e.y <= s.y || e.z <= s.z)
+        return AC_SUCCESS;
+    HaloArgs a;
+    a.L     = L;
+    a.block = d->blk[d->cur];
+    a.lo    = d->lo[d->cur];
+    a.start = s;
+    a.end   = e;
+    a.f0    = f0;
+    a.f1    = f1;
+    a.rows  = (long long)(e.y - s.y) * (e.z - s.z);
+    long long blocks = (a.rows + 7) / 8;
+    blocks           = std::min(blocks, (long long)d->num_sms * 16);
+    halo_kernel<<<(unsigned)blocks, 256, 0, st>>>(a);
+    ACB_CUDA_CHECK(cudaGetLastError());
+    d->launches++;
+    return AC_SUCCESS;
+}
+
+static AcResult
+run_reduce(const Device d, cudaStream_t st, int rtype, int nin, const int* handles,
+           double* result)
+{
+    const Layout& L = d->L;
+    ReduceArgs a;
+    memset(&a, 0, sizeof(a));
+    a.L = L;
+    for (int w = 0; w < nin; ++w) {
+        if (handles[w] < 0 || handles[w] >= NUM_VTXBUF_HANDLES)
+            return AC_FAILURE;
+        a.f[w]  = d->blk[d->cur] + handles[w] * L.fstride;
+        a.lo[w] = d->lo[d->cur] ? d->lo[d->cur] + handles[w] * L.fstride : nullptr;
+    }
+    a.nin      = nin;
+    a.rtype    = rtype;
+    a.start    = make_int3(NGHOST, NGHOST, NGHOST);
+    a.end      = make_int3(NGHOST + L.nx, NGHOST + L.ny, NGHOST + L.nz);
+    a.rows     = (long long)L.ny * L.nz;
+    a.partials = d->red_partials;
+    a.counter  = d->red_counter;
+    a.result   = d->red_result;
+    long long blocks = (a.rows + 7) / 8;
+    blocks           = std::max(1LL, std::min(blocks, (long long)d->red_max_blocks));
+    reduce_kernel<256><<<(unsigned)blocks, 256, 0, st>>>(a);
+    ACB_CUDA_CHECK(cudaGetLastError());
+    d->launches++;
+    ACB_CUDA_CHECK(cudaMemcpyAsync(d->h_result, d->red_result, sizeof(double),
+                                   cudaMemcpyDeviceToHost, st));
+    ACB_CUDA_CHECK(cudaStreamSynchronize(st));
+    *result = *d->h_result;
+    return AC_SUCCESS;
+}
+
+// Visits the rows of a flat range [s, s + count) of logical indices of a field
+// (reference order, rows of mx): fn(dev_offset_elems, flat_offset, n_elems, n_rows)
+// with n_rows > 1 only for runs of whole rows.
+template <class F>
+static AcResult
+for_each_row_run(const Layout& L, size_t s, size_t count, F fn)
+{
+    const size_t mx = (size_t)L.mx;
+    const size_t total = (size_t)L.mx * L.my * L.mz;
+    if (s > total || count > total - s) {
+        fprintf(stderr, "astaroth_b200: transfer range outside the mesh\n");
+        return AC_FAILURE;
+    }
+    size_t t = 0;
+    while (t < count) {
+        const size_t idx = s + t, row = idx / mx, i = idx % mx;
+        const size_t dev = (size_t)L.offx + row * (size_t)L.mxp + i;
+        if (i != 0 || count - t < mx) {
+            const size_t n = std::min(mx - i, count - t);
+            if (fn(dev, t, n, (size_t)1) != AC_SUCCESS)
+                return AC_FAILURE;
+            t += n;
+        }
+        else {
+            const size_t rows = (count - t) / mx;
+            if (fn(dev, t, mx, rows) != AC_SUCCESS)
+                return AC_FAILURE;
+            t += rows * mx;
+        }
+    }
+    return AC_SUCCESS;
+}
+
+static AcResult
+copy_field_range(const Device d, cudaStream_t st, state_t* field, size_t s, AcReal* host,
+                 size_t count, bool h2d, float* lo_field)
+{
+    const Layout& L  = d->L;
+    const size_t w   = sizeof(state_t);
+    const size_t dpw = (size_t)L.mxp * w, hpw = (size_t)L.mx * w;
+    return for_each_row_run(L, s, count, [&](size_t dev, size_t t, size_t n, size_t rows) {
+        cudaError_t err;
+        if (rows == 1)
+            err = h2d ? cudaMemcpyAsync(field + dev, host + t, n * w, cudaMemcpyHostToDevice, st)
+                      : cudaMemcpyAsync(host + t, field + dev, n * w, cudaMemcpyDeviceToHost, st);
+        else
+            err = h2d ? cudaMemcpy2DAsync(field + dev, dpw, host + t, hpw, n * w, rows,
+                                          cudaMemcpyHostToDevice, st)
+                      : cudaMemcpy2DAsync(host + t, hpw, field + dev, dpw, n * w, rows,
+                                          cudaMemcpyDeviceToHost, st);
+        if (err == cudaSuccess && h2d && lo_field) // fresh values carry no lo part
+            err = cudaMemset2DAsync(lo_field + dev, (size_t)L.mxp * sizeof(float), 0,
+                                    n * sizeof(float), rows, st);
+        if (err != cudaSuccess) {
+            fprintf(stderr, "astaroth_b200: transfer failed: %s\n", cudaGetErrorString(err));
+            return AC_FAILURE;
+        }
+        return AC_SUCCESS;
+    });
+}
+
+// flat (reference-order) double <-> padded field, for the double views and fills
+__global__ void
+pack_kernel(const Layout L, state_t* __restrict__ field, float* __restrict__ lo,
+            double* __restrict__ flat, int to_flat, int fill, double value)
+{
+    const long long total = (long long)L.mx * L.my * L.mz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long row = t / L.mx;
+        const int i         = (int)(t - row * L.mx);
+        const long long id  = L.offx + row * L.mxp + i;
+        if (to_flat) {
+            double v = (double)field[id];
+            if (ACB_MIXED && lo)
+                v += (double)lo[id];
+            flat[t] = v;
+        }
+        else {
+            const double v = fill ? value : flat[t];
+            const state_t h = (state_t)v;
+            field[id]       = h;
+            if (ACB_MIXED && lo)
+                lo[id] = (float)(v - (double)h);
+        }
+    }
+}
+
+static AcResult
+launch_pack(const Device d, cudaStream_t st, int blk, int handle, double* flat, int to_flat,
+            int fill, double value)
+{
+    const Layout& L = d->L;
+    state_t* f      = d->blk[blk] + handle * L.fstride;
+    float* lo       = d->lo[blk] ? d->lo[blk] + handle * L.fstride : nullptr;
+    pack_kernel<<<d->num_sms * 8, 256, 0, st>>>(L, f, lo, flat, to_flat, fill, value);
+    ACB_CUDA_CHECK(cudaGetLastError());
+    d->launches++;
+    return AC_SUCCESS;
+}
+
+static AcResult
+ensure_xfer(const Device d)
+{
+    const size_t need = (size_t)d->L.mx * d->L.my * d->L.mz;
+    if (d->xfer && d->xfer_elems >= need)
+        return AC_SUCCESS;
+    if (d->xfer)
+        cudaFree(d->xfer);
+    d->xfer = nullptr;
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->xfer, need * sizeof(double)));
+    d->xfer_elems = need;
+    return AC_SUCCESS;
+}
+
+static void
+invalidate_graphs(const Device d)
+{
+    for (int p = 0; p < 2; ++p) {
+        if (d->graph[p])
+            cudaGraphExecDestroy(d->graph[p]);
+        d->graph[p]     = nullptr;
+        d->graph_key[p] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Interface
+// ---------------------------------------------------------------------------
+extern "C" {
+
+AcResult
+acDevicePrintInfo(const Device device)
+{
+    cudaDeviceProp p;
+    ACB_CUDA_CHECK(cudaGetDeviceProperties(&p, device->id));
+    size_t free_b = 0, total_b = 0;
+    cudaSetDevice(device->id);
+    cudaMemGetInfo(&free_b, &total_b);
+    int n;
+    const SolveConfig* cfgs = solve_configs(&n);
+    printf("--------------------------------------------------\n");
+    printf("Device Number: %d\n", device->id);
+    printf("    Device name: %s\n", p.name);
+    printf("    Compute capability: %d.%d\n", p.major, p.minor);
+    printf("    Multiprocessors: %d\n", p.multiProcessorCount);
+    printf("    Global memory: %.2f GiB (%.2f GiB free)\n", total_b / 1073741824.0,
+           free_b / 1073741824.0);
+    printf("    L2 size: %d KiB\n", p.l2CacheSize / 1024);
+    printf("    Shared memory per block (opt-in): %zu KiB\n", p.sharedMemPerBlockOptin / 1024);
+    printf("  Mesh %d x %d x %d, row pitch %d, %s state\n", device->L.nx, device->L.ny,
+           device->L.nz, device->L.mxp,
+           ACB_MIXED ? "mixed (hi, lo) float" : (sizeof(AcReal) == 8 ? "double" : "float"));
+    printf("  Solve configuration: %s\n", cfgs[device->solve_cfg].name);
+    printf("--------------------------------------------------\n");
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceSynchronizeStream(const Device device, const Stream stream)
+{
+    cudaSetDevice(device->id);
+    if (stream == STREAM_ALL) {
+        ACB_CUDA_CHECK(cudaDeviceSynchronize());
+        unsigned st = 0;
+        ACB_CUDA_CHECK(cudaMemcpy(&st, device->status, sizeof(st), cudaMemcpyDeviceToHost));
+        if (st) {
+            fprintf(stderr, "astaroth_b200: device %d status 0x%x (a kernel gave up waiting)\n",
+                    device->id, st);
+            return AC_FAILURE;
+        }
+    }
+    else {
+        ACB_CUDA_CHECK(cudaStreamSynchronize(stream_of(device, stream)));
+    }
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceLoadScalarUniform(const Device device, const Stream stream, const AcRealParam param,
+                          const AcReal value)
+{
+    (void)stream;
+    if (param < 0 || param >= NUM_REAL_PARAMS) {
+        fprintf(stderr, "WARNING: invalid AcRealParam %d.\n", param);
+        return AC_FAILURE;
+    }
+    if (!real_is_valid((double)value)) {
+        fprintf(stderr, "WARNING: Passed an invalid value %g to device constant %s. Skipping.\n",
+                (double)value, realparam_names[param]);
+        return AC_FAILURE;
+    }
+    if (device->uniforms.real_params[param] != value) {
+        device->uniforms.real_params[param] = value;
+        device->uniform_version++;
+    }
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceLoadVectorUniform(const Device device, const Stream stream, const AcReal3Param param,
+                          const AcReal3 value)
+{
+    (void)device;
+    (void)stream;
+    (void)value;
+    // the module declares no vector uniforms (NUM_REAL3_PARAMS == 0)
+    fprintf(stderr, "WARNING: invalid AcReal3Param %d\n", (int)param);
+    return AC_FAILURE;
+}
+
+AcResult
+acDeviceLoadIntUniform(const Device device, const Stream stream, const AcIntParam param,
+                       const int value)
+{
+    (void)stream;
+    if (param < 0 || param >= NUM_INT_PARAMS) {
+        fprintf(stderr, "WARNING: invalid AcIntParam %d\n", param);
+        return AC_FAILURE;
+    }
+    device->uniforms.int_params[param] = value;
+    device->uniform_version++;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceLoadInt3Uniform(const Device device, const Stream stream, const AcInt3Param param,
+                        const int3 value)
+{
+    (void)stream;
+    if (param < 0 || param >= NUM_INT3_PARAMS) {
+        fprintf(stderr, "WARNING: invalid AcInt3Param %d\n", param);
+        return AC_FAILURE;
+    }
+    device->uniforms.int3_params[param] = value;
+    device->uniform_version++;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceLoadScalarArray(const Device device, const Stream stream, const ScalarArrayHandle handle,
+                        const size_t start, const AcReal* data, const size_t num)
+{
+    (void)device;
+    (void)stream;
+    (void)handle;
+    (void)start;
+    (void)data;
+    (void)num;
+    return AC_FAILURE; // the module declares no scalar arrays
+}
+
+AcResult
+acDeviceLoadMeshInfo(const Device device, const AcMeshInfo config)
+{
+    const int* a = config.int_params;
+    const int* b = device->local_config.int_params;
+    if (a[AC_nx] != b[AC_nx] || a[AC_ny] != b[AC_ny] || a[AC_nz] != b[AC_nz] ||
+        config.int3_params[AC_multigpu_offset].x !=
+            device->local_config.int3_params[AC_multigpu_offset].x ||
+        config.int3_params[AC_multigpu_offset].y !=
+            device->local_config.int3_params[AC_multigpu_offset].y ||
+        config.int3_params[AC_multigpu_offset].z !=
+            device->local_config.int3_params[AC_multigpu_offset].z) {
+        fprintf(stderr, "astaroth_b200: acDeviceLoadMeshInfo with other dimensions\n");
+        return AC_FAILURE;
+    }
+    for (int i = 0; i < NUM_INT_PARAMS; ++i)
+        acDeviceLoadIntUniform(device, STREAM_DEFAULT, (AcIntParam)i, config.int_params[i]);
+    for (int i = 0; i < NUM_INT3_PARAMS; ++i)
+        acDeviceLoadInt3Uniform(device, STREAM_DEFAULT, (AcInt3Param)i, config.int3_params[i]);
+    for (int i = 0; i < NUM_REAL_PARAMS; ++i)
+        if (real_is_valid((double)config.real_params[i]))
+            acDeviceLoadScalarUniform(device, STREAM_DEFAULT, (AcRealParam)i,
+                                      config.real_params[i]);
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceLoadDefaultUniforms(const Device device)
+{
+    // Defaults of the module's uniforms: zero unless the module gives a value
+    // (acc/stdlib/stdderiv.h:6-11, acc/mhd_solver/stencil_kernel.ac:69,112).
+    memset(&device->uniforms, 0, sizeof(device->uniforms));
+    AcReal* rp          = device->uniforms.real_params;
+    const AcReal ds     = (AcReal)0.04908738521;
+    rp[AC_dsx]          = ds;
+    rp[AC_dsy]          = ds;
+    rp[AC_dsz]          = ds;
+    rp[AC_inv_dsx]      = (AcReal)1.0 / ds;
+    rp[AC_inv_dsy]      = (AcReal)1.0 / ds;
+    rp[AC_inv_dsz]      = (AcReal)1.0 / ds;
+    rp[AC_cs_sound]     = (AcReal)1.0;
+    rp[AC_cs2_sound]    = rp[AC_cs_sound] * rp[AC_cs_sound];
+    device->uniform_version++;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceCreate(const int id, const AcMeshInfo config, Device* device_handle)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || id < 0 || id >= ndev) {
+        fprintf(stderr, "astaroth_b200: no CUDA device %d\n", id);
+        return AC_FAILURE;
+    }
+    const int nx = config.int_params[AC_nx], ny = config.int_params[AC_ny],
+              nz = config.int_params[AC_nz];
+    if (nx < NGHOST || ny < NGHOST || nz < NGHOST) {
+        fprintf(stderr, "astaroth_b200: mesh %d x %d x %d too small\n", nx, ny, nz);
+        return AC_FAILURE;
+    }
+    ACB_CUDA_CHECK(cudaSetDevice(id));
+    struct device_s* d = (struct device_s*)calloc(1, sizeof(struct device_s));
+    if (!d)
+        return AC_FAILURE;
+    d->id           = id;
+    d->local_config = config;
+    d->tmap_cfg     = -1;
+    d->solve_cfg    = kDefaultSolveConfig;
+    ACB_CUDA_CHECK(cudaDeviceGetAttribute(&d->num_sms, cudaDevAttrMultiProcessorCount, id));
+
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    for (int i = 0; i < NUM_STREAMS; ++i) {
+        int prio = prio_lo - i; // stream 0 lowest priority, as the reference's 0..31 clamped
+        if (prio < prio_hi)
+            prio = prio_hi;
+        ACB_CUDA_CHECK(cudaStreamCreateWithPriority(&d->streams[i], cudaStreamNonBlocking, prio));
+    }
+
+    d->L               = make_layout(nx, ny, nz, (int)sizeof(state_t));
+    const size_t bytes = (size_t)d->L.fstride * ACB_NF * sizeof(state_t);
+    for (int b = 0; b < 2; ++b) {
+        ACB_CUDA_CHECK(cudaMalloc((void**)&d->blk[b], bytes));
+        ACB_CUDA_CHECK(cudaMemset(d->blk[b], 0, bytes));
+#if ACB_MIXED
+        ACB_CUDA_CHECK(cudaMalloc((void**)&d->lo[b], (size_t)d->L.fstride * ACB_NF * sizeof(float)));
+        ACB_CUDA_CHECK(cudaMemset(d->lo[b], 0, (size_t)d->L.fstride * ACB_NF * sizeof(float)));
+#endif
+    }
+    d->red_max_blocks = d->num_sms * 8;
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_partials, sizeof(double) * d->red_max_blocks));
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_counter, sizeof(unsigned)));
+    ACB_CUDA_CHECK(cudaMemset(d->red_counter, 0, sizeof(unsigned)));
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_result, sizeof(double)));
+    ACB_CUDA_CHECK(cudaMallocHost((void**)&d->h_result, sizeof(double)));
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->status, sizeof(unsigned)));
+    ACB_CUDA_CHECK(cudaMemset(d->status, 0, sizeof(unsigned)));
+
+    acDeviceLoadDefaultUniforms(d);
+    acDeviceLoadMeshInfo(d, config);
+    if (prepare_kernels_once() != AC_SUCCESS)
+        return AC_FAILURE;
+    ACB_CUDA_CHECK(cudaDeviceSynchronize());
+    *device_handle = d;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceDestroy(Device device)
+{
+    if (!device)
+        return AC_FAILURE;
+    cudaSetDevice(device->id);
+    cudaDeviceSynchronize();
+    invalidate_graphs(device);
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(device->blk[b]);
+        if (device->lo[b])
+            cudaFree(device->lo[b]);
+    }
+    cudaFree(device->red_partials);
+    cudaFree(device->red_counter);
+    cudaFree(device->red_result);
+    cudaFreeHost(device->h_result);
+    cudaFree(device->status);
+    if (device->xfer)
+        cudaFree(device->xfer);
+    for (int i = 0; i < NUM_STREAMS; ++i)
+        cudaStreamDestroy(device->streams[i]);
+    free(device);
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceAutoOptimize(const Device device)
+{
+    // Times every compiled tile configuration on one full-domain substep (s = 1)
+    // and keeps the fastest; the buffers are restored afterwards.
+    cudaSetDevice(device->id);
+    int n;
+    solve_configs(&n);
+    const cudaStream_t st = device->streams[STREAM_DEFAULT];
+    const int3 s          = make_int3(NGHOST, NGHOST, NGHOST);
+    const int3 e = make_int3(NGHOST + device->L.nx, NGHOST + device->L.ny, NGHOST + device->L.nz);
+    // keep the out block (the substep overwrites it)
+    const size_t bytes = (size_t)device->L.fstride * ACB_NF * sizeof(state_t);
+    state_t* save      = nullptr;
+    ACB_CUDA_CHECK(cudaMalloc((void**)&save, bytes));
+    ACB_CUDA_CHECK(cudaMemcpyAsync(save, device->blk[device->cur ^ 1], bytes,
+                                   cudaMemcpyDeviceToDevice, st));
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    const int saved_cfg = device->solve_cfg;
+    int best            = saved_cfg;
+    float best_ms       = INFINITY;
+    for (int c = 0; c < n; ++c) {
+        device->solve_cfg = c;
+        if (launch_solve(device, st, 1, s, e) != AC_SUCCESS) // warm-up
+            continue;
+        cudaEventRecord(t0, st);
+        const int reps = 3;
+        for (int r = 0; r < reps; ++r)
+            launch_solve(device, st, 1, s, e);
+        cudaEventRecord(t1, st);
+        cudaEventSynchronize(t1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, t0, t1);
+        if (cudaGetLastError() == cudaSuccess && ms < best_ms) {
+            best_ms = ms;
+            best    = c;
+        }
+    }
+    device->solve_cfg = best;
+    ACB_CUDA_CHECK(cudaMemcpyAsync(device->blk[device->cur ^ 1], save, bytes,
+                                   cudaMemcpyDeviceToDevice, st));
+    ACB_CUDA_CHECK(cudaStreamSynchronize(st));
+    cudaFree(save);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    invalidate_graphs(device);
+    (void)saved_cfg;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceSwapBuffers(const Device device)
+{
+    device->cur ^= 1;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceLoadVertexBufferWithOffset(const Device device, const Stream stream,
+                                   const AcMesh host_mesh, const VertexBufferHandle h,
+                                   const int3 src, const int3 dst, const int num_vertices)
+{
+    if (h < 0 || h >= NUM_VTXBUF_HANDLES || num_vertices < 0)
+        return AC_FAILURE;
+    cudaSetDevice(device->id);
+    const size_t sidx = acVertexBufferIdx(src.x, src.y, src.z, host_mesh.info);
+    const size_t didx = acVertexBufferIdx(dst.x, dst.y, dst.z, device->local_config);
+    const Layout& L   = device->L;
+    float* lo         = device->lo[device->cur] ? device->lo[device->cur] + h * L.fstride : nullptr;
+    return copy_field_range(device, stream_of(device, stream),
+                            device->blk[device->cur] + h * L.fstride, didx,
+                            host_mesh.vertex_buffer[h] + sidx, (size_t)num_vertices, true, lo);
+}
+
+AcResult
+acDeviceLoadMeshWithOffset(const Device device, const Stream stream, const AcMesh host_mesh,
+                           const int3 src, const int3 dst, const int num_vertices)
+{
+    for (int i = 0; i < NUM_VTXBUF_HANDLES; ++i)
+        if (acDeviceLoadVertexBufferWithOffset(device, stream, host_mesh, (VertexBufferHandle)i,
+                                               src, dst, num_vertices) != AC_SUCCESS)
+            return AC_FAILURE;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceLoadVertexBuffer(const Device device, const Stream stream, const AcMesh host_mesh,
+                         const VertexBufferHandle h)
+{
+    const int3 z = make_int3(0, 0, 0);
+    return acDeviceLoadVertexBufferWithOffset(device, stream, host_mesh, h, z, z,
+                                              (int)acVertexBufferSize(device->local_config));
+}
+
+AcResult
+acDeviceLoadMesh(const Device device, const Stream stream, const AcMesh host_mesh)
+{
+    for (int i = 0; i < NUM_VTXBUF_HANDLES; ++i)
+        if (acDeviceLoadVertexBuffer(device, stream, host_mesh, (VertexBufferHandle)i) !=
+            AC_SUCCESS)
+            return AC_FAILURE;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceSetVertexBuffer(const Device device, const Stream stream, const VertexBufferHandle h,
+                        const AcReal value)
+{
+    if (h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    cudaSetDevice(device->id);
+    const cudaStream_t st = stream_of(device, stream);
+    // both in and out, as the reference does (src/core/device.cc:296-314)
+    for (int b = 0; b < 2; ++b)
+        if (launch_pack(device, st, b, h, nullptr, 0, 1, (double)value) != AC_SUCCESS)
+            return AC_FAILURE;
+    ACB_CUDA_CHECK(cudaStreamSynchronize(st));
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceStoreVertexBufferWithOffset(const Device device, const Stream stream,
+                                    const VertexBufferHandle h, const int3 src, const int3 dst,
+                                    const int num_vertices, AcMesh* host_mesh)
+{
+    if (h < 0 || h >= NUM_VTXBUF_HANDLES || num_vertices < 0)
+        return AC_FAILURE;
+    cudaSetDevice(device->id);
+    const size_t sidx = acVertexBufferIdx(src.x, src.y, src.z, device->local_config);
+    const size_t didx = acVertexBufferIdx(dst.x, dst.y, dst.z, host_mesh->info);
+    const Layout& L   = device->L;
+    return copy_field_range(device, stream_of(device, stream),
+                            device->blk[device->cur] + h * L.fstride, sidx,
+                            host_mesh->vertex_buffer[h] + didx, (size_t)num_vertices, false,
+                            nullptr);
+}
+
+AcResult
+acDeviceStoreMeshWithOffset(const Device device, const Stream stream, const int3 src,
+                            const int3 dst, const int num_vertices, AcMesh* host_mesh)
+{
+    for (int i = 0; i < NUM_VTXBUF_HANDLES; ++i)
+        if (acDeviceStoreVertexBufferWithOffset(device, stream, (VertexBufferHandle)i, src, dst,
+                                                num_vertices, host_mesh) != AC_SUCCESS)
+            return AC_FAILURE;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceStoreVertexBuffer(const Device device, const Stream stream, const VertexBufferHandle h,
+                          AcMesh* host_mesh)
+{
+    const int3 z = make_int3(0, 0, 0);
+    return acDeviceStoreVertexBufferWithOffset(device, stream, h, z, z,
+                                               (int)acVertexBufferSize(device->local_config),
+                                               host_mesh);
+}
+
+AcResult
+acDeviceStoreMesh(const Device device, const Stream stream, AcMesh* host_mesh)
+{
+    for (int i = 0; i < NUM_VTXBUF_HANDLES; ++i)
+        if (acDeviceStoreVertexBuffer(device, stream, (VertexBufferHandle)i, host_mesh) !=
+            AC_SUCCESS)
+            return AC_FAILURE;
+    return AC_SUCCESS;
+}
+
+// device-to-device flat-range copy between two padded layouts
+__global__ void
+transfer_kernel(const Layout Ls, const state_t* __restrict__ src, long long s0, const Layout Ld,
+                state_t* __restrict__ dst, long long d0, long long count)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long a = s0 + t, b = d0 + t;
+        const long long ra = a / Ls.mx, rb = b / Ld.mx;
+        dst[Ld.offx + rb * Ld.mxp + (b - rb * Ld.mx)] = src[Ls.offx + ra * Ls.mxp + (a - ra * Ls.mx)];
+    }
+}
+
+AcResult
+acDeviceTransferVertexBufferWithOffset(const Device src_device, const Stream stream,
+                                       const VertexBufferHandle h, const int3 src,
+                                       const int3 dst, const int num_vertices, Device dst_device)
+{
+    if (h < 0 || h >= NUM_VTXBUF_HANDLES || num_vertices < 0)
+        return AC_FAILURE;
+    const size_t sidx = acVertexBufferIdx(src.x, src.y, src.z, src_device->local_config);
+    const size_t didx = acVertexBufferIdx(dst.x, dst.y, dst.z, dst_device->local_config);
+    const size_t st   = acVertexBufferSize(src_device->local_config);
+    const size_t dt   = acVertexBufferSize(dst_device->local_config);
+    if (sidx + num_vertices > st || didx + num_vertices > dt)
+        return AC_FAILURE;
+    if (src_device->id != dst_device->id) {
+        fprintf(stderr, "astaroth_b200: transfers between GPUs are not supported\n");
+        return AC_FAILURE;
+    }
+    cudaSetDevice(src_device->id);
+    transfer_kernel<<<src_device->num_sms * 4, 256, 0, stream_of(src_device, stream)>>>(
+        src_device->L, src_device->blk[src_device->cur] + h * src_device->L.fstride,
+        (long long)sidx, dst_device->L, dst_device->blk[dst_device->cur] + h * dst_device->L.fstride,
+        (long long)didx, (long long)num_vertices);
+    ACB_CUDA_CHECK(cudaGetLastError());
+    src_device->launches++;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceTransferMeshWithOffset(const Device src_device, const Stream stream, const int3 src,
+                               const int3 dst, const int num_vertices, Device* dst_device)
+{
+    for (int i = 0; i < NUM_VTXBUF_HANDLES; ++i)
+        if (acDeviceTransferVertexBufferWithOffset(src_device, stream, (VertexBufferHandle)i, src,
+                                                   dst, num_vertices, *dst_device) != AC_SUCCESS)
+            return AC_FAILURE;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceTransferVertexBuffer(const Device src_device, const Stream stream,
+                             const VertexBufferHandle h, Device dst_device)
+{
+    const int3 z = make_int3(0, 0, 0);
+    return acDeviceTransferVertexBufferWithOffset(src_device, stream, h, z, z,
+                                                  (int)acVertexBufferSize(src_device->local_config),
+                                                  dst_device);
+}
+
+AcResult
+acDeviceTransferMesh(const Device src_device, const Stream stream, Device dst_device)
+{
+    for (int i = 0; i < NUM_VTXBUF_HANDLES; ++i)
+        if (acDeviceTransferVertexBuffer(src_device, stream, (VertexBufferHandle)i, dst_device) !=
+            AC_SUCCESS)
+            return AC_FAILURE;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceIntegrateSubstep(const Device device, const Stream stream, const int step_number,
+                         const int3 start, const int3 end, const AcReal dt)
+{
+    cudaSetDevice(device->id);
+    if (acDeviceLoadScalarUniform(device, stream, AC_dt, dt) != AC_SUCCESS)
+        return AC_FAILURE;
+    return launch_solve(device, stream_of(device, stream), step_number, start, end);
+}
+
+AcResult
+acDevicePeriodicBoundcondStep(const Device device, const Stream stream,
+                              const VertexBufferHandle h, const int3 start, const int3 end)
+{
+    if (h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    cudaSetDevice(device->id);
+    return launch_halo(device, stream_of(device, stream), start, end, (int)h, (int)h + 1);
+}
+
+AcResult
+acDevicePeriodicBoundconds(const Device device, const Stream stream, const int3 start,
+                           const int3 end)
+{
+    cudaSetDevice(device->id);
+    return launch_halo(device, stream_of(device, stream), start, end, 0, NUM_VTXBUF_HANDLES);
+}
+
+AcResult
+acDeviceGeneralBoundcondStep(const Device device, const Stream stream,
+                             const VertexBufferHandle h, const int3 start, const int3 end,
+                             const AcMeshInfo config, const int3 bindex)
+{
+    (void)bindex;
+    // The reference dispatches on the x-top condition only
+    // (src/core/kernels/boundconds.cuh:192-242); its symmetric kernels write
+    // sign*src*0 + 1 (:127) and are not reproduced.
+    const int bc = config.int_params[AC_bc_type_top_x];
+    if (bc == AC_BOUNDCOND_PERIODIC)
+        return acDevicePeriodicBoundcondStep(device, stream, h, start, end);
+    fprintf(stderr, "ERROR: Boundary condition %d not supported (periodic only)\n", bc);
+    return AC_FAILURE;
+}
+
+AcResult
+acDeviceGeneralBoundconds(const Device device, const Stream stream, const int3 start,
+                          const int3 end, const AcMeshInfo config, const int3 bindex)
+{
+    for (int i = 0; i < NUM_VTXBUF_HANDLES; ++i)
+        if (acDeviceGeneralBoundcondStep(device, stream, (VertexBufferHandle)i, start, end, config,
+                                         bindex) != AC_SUCCESS)
+            return AC_FAILURE;
+    return AC_SUCCESS;
+}
+
+static bool
+rtype_ok(int rtype, int nin)
+{
+    if (nin == RED_ALFVEN)
+        return rtype == RTYPE_ALFVEN_MAX || rtype == RTYPE_ALFVEN_MIN || rtype == RTYPE_ALFVEN_RMS;
+    return rtype == RTYPE_MAX || rtype == RTYPE_MIN || rtype == RTYPE_RMS ||
+           rtype == RTYPE_RMS_EXP || rtype == RTYPE_SUM;
+}
+
+AcResult
+acDeviceReduceScalDouble(const Device device, const Stream stream, const ReductionType rtype,
+                         const VertexBufferHandle h, double* result)
+{
+    if (!rtype_ok(rtype, RED_SCAL)) {
+        fprintf(stderr, "astaroth_b200: unsupported reduction type %d\n", (int)rtype);
+        *result = NAN;
+        return AC_FAILURE;
+    }
+    cudaSetDevice(device->id);
+    const int hs[1] = {(int)h};
+    return run_reduce(device, stream_of(device, stream), rtype, RED_SCAL, hs, result);
+}
+
+AcResult
+acDeviceReduceVecDouble(const Device device, const Stream stream, const ReductionType rtype,
+                        const VertexBufferHandle a, const VertexBufferHandle b,
+                        const VertexBufferHandle c, double* result)
+{
+    if (!rtype_ok(rtype, RED_VEC)) {
+        fprintf(stderr, "astaroth_b200: unsupported reduction type %d\n", (int)rtype);
+        *result = NAN;
+        return AC_FAILURE;
+    }
+    cudaSetDevice(device->id);
+    const int hs[3] = {(int)a, (int)b, (int)c};
+    return run_reduce(device, stream_of(device, stream), rtype, RED_VEC, hs, result);
+}
+
+AcResult
+acDeviceReduceScal(const Device device, const Stream stream, const ReductionType rtype,
+                   const VertexBufferHandle h, AcReal* result)
+{
+    double r      = NAN;
+    AcResult rc   = acDeviceReduceScalDouble(device, stream, rtype, h, &r);
+    *result       = (AcReal)r;
+    return rc;
+}
+
+AcResult
+acDeviceReduceVec(const Device device, const Stream stream, const ReductionType rtype,
+                  const VertexBufferHandle a, const VertexBufferHandle b,
+                  const VertexBufferHandle c, AcReal* result)
+{
+    double r    = NAN;
+    AcResult rc = acDeviceReduceVecDouble(device, stream, rtype, a, b, c, &r);
+    *result     = (AcReal)r;
+    return rc;
+}
+
+AcResult
+acDeviceReduceVecScal(const Device device, const Stream stream, const ReductionType rtype,
+                      const VertexBufferHandle a, const VertexBufferHandle b,
+                      const VertexBufferHandle c, const VertexBufferHandle d, AcReal* result)
+{
+    if (!rtype_ok(rtype, RED_ALFVEN)) {
+        fprintf(stderr, "astaroth_b200: unsupported reduction type %d\n", (int)rtype);
+        *result = (AcReal)NAN;
+        return AC_FAILURE;
+    }
+    cudaSetDevice(device->id);
+    const int hs[4] = {(int)a, (int)b, (int)c, (int)d};
+    double r        = NAN;
+    AcResult rc     = run_reduce(device, stream_of(device, stream), rtype, RED_ALFVEN, hs, &r);
+    *result         = (AcReal)r;
+    return rc;
+}
+
+AcResult
+acDeviceRunMPITest(void)
+{
+    fprintf(stderr, "astaroth_b200: acDeviceRunMPITest: no MPI layer in this build\n");
+    return AC_FAILURE;
+}
+
+// ---------------------------------------------------------------------------
+// additions (include/astaroth_b200.h)
+// ---------------------------------------------------------------------------
+AcResult
+acDeviceGetStatus(const Device device, unsigned* status)
+{
+    cudaSetDevice(device->id);
+    ACB_CUDA_CHECK(cudaDeviceSynchronize());
+    ACB_CUDA_CHECK(cudaMemcpy(status, device->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceGetCudaStream(const Device device, const Stream stream, void** cuda_stream)
+{
+    *cuda_stream = (void*)stream_of(device, stream);
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceGetLaunchCount(const Device device, unsigned long long* count)
+{
+    *count = device->launches;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceSetSolveConfig(const Device device, const int config)
+{
+    int n;
+    solve_configs(&n);
+    const int c = config < 0 ? kDefaultSolveConfig : config;
+    if (c >= n)
+        return AC_FAILURE;
+    if (device->solve_cfg != c) {
+        device->solve_cfg = c;
+        invalidate_graphs(device);
+    }
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceGetSolveConfig(const Device device, int* config, int* num_configs)
+{
+    solve_configs(num_configs);
+    *config = device->solve_cfg;
+    return AC_SUCCESS;
+}
+
+const char*
+acSolveConfigName(const int config)
+{
+    int n;
+    const SolveConfig* cfgs = solve_configs(&n);
+    return (config >= 0 && config < n) ? cfgs[config].name : "invalid";
+}
+
+AcResult
+acDeviceGetMemoryFootprint(const Device device, size_t* bytes)
+{
+    size_t b = 2 * (size_t)device->L.fstride * ACB_NF * sizeof(state_t);
+    if (device->lo[0])
+        b += 2 * (size_t)device->L.fstride * ACB_NF * sizeof(float);
+    *bytes = b;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceSetForcing(const Device device, const int enabled)
+{
+    device->forcing = enabled ? 1 : 0;
+    device->uniform_version++;
+    return AC_SUCCESS;
+}
+
+static AcResult
+enqueue_step(const Device d, cudaStream_t st)
+{
+    const int3 m0 = make_int3(0, 0, 0);
+    const int3 m1 = make_int3(d->L.mx, d->L.my, d->L.mz);
+    const int3 n0 = make_int3(NGHOST, NGHOST, NGHOST);
+    const int3 n1 = make_int3(NGHOST + d->L.nx, NGHOST + d->L.ny, NGHOST + d->L.nz);
+    for (int s = 0; s < 3; ++s) {
+        if (launch_halo(d, st, m0, m1, 0, NUM_VTXBUF_HANDLES) != AC_SUCCESS)
+            return AC_FAILURE;
+        if (launch_solve(d, st, s, n0, n1) != AC_SUCCESS)
+            return AC_FAILURE;
+        d->cur ^= 1;
+    }
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceIntegrateStep(const Device device, const Stream stream, const AcReal dt)
+{
+    cudaSetDevice(device->id);
+    if (acDeviceLoadScalarUniform(device, stream, AC_dt, dt) != AC_SUCCESS)
+        return AC_FAILURE;
+    return enqueue_step(device, stream_of(device, stream));
+}
+
+AcResult
+acDeviceIntegrateSteps(const Device device, const Stream stream, const AcReal dt,
+                       const int num_steps)
+{
+    cudaSetDevice(device->id);
+    if (num_steps <= 0)
+        return AC_SUCCESS;
+    if (acDeviceLoadScalarUniform(device, stream, AC_dt, dt) != AC_SUCCESS)
+        return AC_FAILURE;
+    if (prepare_kernels_once() != AC_SUCCESS || ensure_maps(device) != AC_SUCCESS)
+        return AC_FAILURE;
+    const cudaStream_t st = stream_of(device, stream);
+    // key: parameters, configuration and stream the graph was captured with
+    const unsigned long long key = (device->uniform_version << 8) ^
+                                   ((unsigned long long)device->solve_cfg << 1) ^
+                                   ((unsigned long long)stream << 40) ^ 1ull;
+    for (int i = 0; i < num_steps; ++i) {
+        const int p = device->cur;
+        if (!device->graph[p] || device->graph_key[p] != key) {
+            if (device->graph[p])
+                cudaGraphExecDestroy(device->graph[p]);
+            device->graph[p] = nullptr;
+            cudaGraph_t g;
+            ACB_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            const unsigned long long before = device->launches;
+            const AcResult rc               = enqueue_step(device, st);
+            ACB_CUDA_CHECK(cudaStreamEndCapture(st, &g));
+            device->cur      = p; // capture advanced the roles; replay does it below
+            device->launches = before;
+            if (rc != AC_SUCCESS) {
+                cudaGraphDestroy(g);
+                return AC_FAILURE;
+            }
+            ACB_CUDA_CHECK(cudaGraphInstantiate(&device->graph[p], g, 0));
+            cudaGraphDestroy(g);
+            device->graph_key[p] = key;
+        }
+        ACB_CUDA_CHECK(cudaGraphLaunch(device->graph[p], st));
+        device->launches += 6;
+        device->cur ^= 1; // three swaps per step
+    }
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceLoadVertexBufferDouble(const Device device, const Stream stream,
+                               const VertexBufferHandle h, const double* src)
+{
+    if (h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    cudaSetDevice(device->id);
+    if (ensure_xfer(device) != AC_SUCCESS)
+        return AC_FAILURE;
+    const cudaStream_t st = stream_of(device, stream);
+    const size_t n        = (size_t)device->L.mx * device->L.my * device->L.mz;
+    ACB_CUDA_CHECK(cudaMemcpyAsync(device->xfer, src, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (launch_pack(device, st, device->cur, h, device->xfer, 0, 0, 0.0) != AC_SUCCESS)
+        return AC_FAILURE;
+    ACB_CUDA_CHECK(cudaStreamSynchronize(st));
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceStoreVertexBufferDouble(const Device device, const Stream stream,
+                                const VertexBufferHandle h, double* dst)
+{
+    if (h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    cudaSetDevice(device->id);
+    if (ensure_xfer(device) != AC_SUCCESS)
+        return AC_FAILURE;
+    const cudaStream_t st = stream_of(device, stream);
+    const size_t n        = (size_t)device->L.mx * device->L.my * device->L.mz;
+    if (launch_pack(device, st, device->cur, h, device->xfer, 1, 0, 0.0) != AC_SUCCESS)
+        return AC_FAILURE;
+    ACB_CUDA_CHECK(cudaMemcpyAsync(dst, device->xfer, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ACB_CUDA_CHECK(cudaStreamSynchronize(st));
+    return AC_SUCCESS;
+}
+
+} // extern "C"

@@ -1,0 +1,157 @@
+// Single-pass reductions over the interior: MAX, MIN, RMS (raw sum of
+// squares), RMS_EXP (raw sum of exp^2), SUM, for one field, a vector of three
+// fields (by length), or the Alfven speed of three fields plus a density.
+//
+// Reference behaviour (src/core/kernels/reductions.cuh:18-343, device layer
+// src/core/device.cc:477-537): filter functions
+//     scalar  v, v^2, exp(v)^2
+//     vector  |v|, |v|^2, sum_i exp(v_i)^2         (SUM of a vector sums |v|)
+//     Alfven  |B| / sqrt(4 pi exp(rho)),  |B|^2 / (4 pi exp(rho))
+// over [n_min, n_max); the device layer returns the unnormalised sum for RMS
+// and RMS_EXP.
+//
+// The reference runs a filter kernel into an n^3 scratch array, a 128-wide
+// shared-memory tree, then a single thread folding n^3/128 partials serially,
+// all accumulating in AcReal. Here: one kernel, one read of each input; per
+// thread FP64 accumulation over warp-owned rows, a warp-shuffle tree, a block
+// tree, one FP64 partial per block in scratch, and the last block to finish
+// folds the partials in a fixed order (deterministic, no atomics on data).
+#pragma once
+#include "common.cuh"
+
+enum { RED_SCAL = 1, RED_VEC = 3, RED_ALFVEN = 4 };
+
+struct ReduceArgs {
+    Layout L;
+    const state_t* f[4];
+    const float* lo[4]; // mixed build: lo parts (else null)
+    int nin;            // 1, 3 or 4
+    int rtype;          // ReductionType
+    int3 start, end;
+    long long rows;
+    double* partials;   // gridDim.x doubles of scratch
+    unsigned* counter;  // scratch counter, zero between launches
+    double* result;
+};
+
+__device__ __forceinline__ double
+red_combine(int rtype, double a, double b)
+{
+    if (rtype == RTYPE_MAX || rtype == RTYPE_ALFVEN_MAX)
+        return fmax(a, b);
+    if (rtype == RTYPE_MIN || rtype == RTYPE_ALFVEN_MIN)
+        return fmin(a, b);
+    return a + b;
+}
+
+__device__ __forceinline__ double
+red_identity(int rtype)
+{
+    if (rtype == RTYPE_MAX || rtype == RTYPE_ALFVEN_MAX)
+        return -INFINITY;
+    if (rtype == RTYPE_MIN || rtype == RTYPE_ALFVEN_MIN)
+        return INFINITY;
+    return 0.0;
+}
+
+__device__ __forceinline__ double
+red_load(const ReduceArgs& a, int w, long long id)
+{
+    double v = (double)a.f[w][id];
+#if ACB_MIXED
+    v += (double)a.lo[w][id];
+#endif
+    return v;
+}
+
+__device__ __forceinline__ double
+red_filter(const ReduceArgs& a, long long id)
+{
+    const int rt = a.rtype;
+    if (a.nin == RED_SCAL) {
+        const double v = red_load(a, 0, id);
+        if (rt == RTYPE_RMS)
+            return v * v;
+        if (rt == RTYPE_RMS_EXP) {
+            const double e = exp(v);
+            return e * e;
+        }
+        return v; // MAX, MIN, SUM
+    }
+    const double x = red_load(a, 0, id), y = red_load(a, 1, id), z = red_load(a, 2, id);
+    if (a.nin == RED_VEC) {
+        if (rt == RTYPE_RMS)
+            return x * x + y * y + z * z;
+        if (rt == RTYPE_RMS_EXP) {
+            const double ex = exp(x), ey = exp(y), ez = exp(z);
+            return ex * ex + ey * ey + ez * ez;
+        }
+        return sqrt(x * x + y * y + z * z); // MAX, MIN, SUM of the length
+    }
+    // Alfven speed with density exponent d
+    const double d  = red_load(a, 3, id);
+    const double b2 = x * x + y * y + z * z;
+    const double q  = 4.0 * M_PI * exp(d);
+    if (rt == RTYPE_ALFVEN_RMS)
+        return b2 / q;
+    return sqrt(b2) / sqrt(q);
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS)
+reduce_kernel(const ReduceArgs a)
+{
+    const Layout& L = a.L;
+    const int lane  = threadIdx.x & 31;
+    const int wid   = threadIdx.x >> 5;
+    const long long gw  = ((long long)blockIdx.x * THREADS + threadIdx.x) >> 5;
+    const long long nw  = ((long long)gridDim.x * THREADS) >> 5;
+    const int rx        = a.end.x - a.start.x;
+    const int ry        = a.end.y - a.start.y;
+    double acc          = red_identity(a.rtype);
+    for (long long r = gw; r < a.rows; r += nw) {
+        const int j          = a.start.y + (int)(r % ry);
+        const int k          = a.start.z + (int)(r / ry);
+        const long long base = lidx(L, a.start.x, j, k);
+        for (int i = lane; i < rx; i += 32)
+            acc = red_combine(a.rtype, acc, red_filter(a, base + i));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        acc = red_combine(a.rtype, acc, __shfl_xor_sync(0xffffffffu, acc, o));
+    __shared__ double wsum[THREADS / 32];
+    __shared__ bool last;
+    if (lane == 0)
+        wsum[wid] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = wsum[0];
+        for (int w = 1; w < THREADS / 32; ++w)
+            b = red_combine(a.rtype, b, wsum[w]);
+        a.partials[blockIdx.x] = b;
+        __threadfence();
+        const unsigned done = atomicAdd(a.counter, 1u);
+        last                = (done == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) {
+        // fixed-order fold of the partials: lanes stride, then a fixed tree
+        __threadfence();
+        double v = red_identity(a.rtype);
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += THREADS)
+            v = red_combine(a.rtype, v, ((volatile double*)a.partials)[b]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            v = red_combine(a.rtype, v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0)
+            wsum[wid] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b = wsum[0];
+            for (int w = 1; w < THREADS / 32; ++w)
+                b = red_combine(a.rtype, b, wsum[w]);
+            *a.result  = b;
+            *a.counter = 0u; // ready for the next launch on this stream
+        }
+    }
+}

@@ -1,0 +1,191 @@
+"""Python host mirror of the reference's Device interface (include/astaroth.h
+acDevice*, reference src/core/device.cc). Each method is a thin call through
+the C ABI of the in-tree library; a non-zero AcResult raises AcError.
+
+    dev = Device("sp", info)
+    dev.load_mesh(host)                 # acDeviceLoadMesh
+    for s in range(3):
+        dev.periodic_boundconds()       # acDevicePeriodicBoundconds
+        dev.integrate_substep(s, dt)    # acDeviceIntegrateSubstep
+        dev.swap_buffers()              # acDeviceSwapBuffers
+    umax = dev.reduce_vec(abi.RTYPE_MAX, abi.VTXBUF_UUX, abi.VTXBUF_UUY, abi.VTXBUF_UUZ)
+    dev.store_mesh(host)
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi, library
+
+
+class AcError(RuntimeError):
+    pass
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != abi.AC_SUCCESS:
+        raise AcError(f"{what} returned AC_FAILURE")
+
+
+def i3(x: int, y: int, z: int) -> abi.int3:
+    return abi.int3(int(x), int(y), int(z))
+
+
+class Device:
+    def __init__(self, flavour: str, info, device_id: int = 0):
+        self.flavour = flavour
+        self.prec = abi.PRECISIONS[flavour]
+        self.lib = library.load(flavour)
+        self.info = info
+        self.n = abi.dims(info)
+        self.handle = C.c_void_p()
+        _check(self.lib.acDeviceCreate(device_id, info, C.byref(self.handle)), "acDeviceCreate")
+
+    # --- lifetime ---------------------------------------------------------
+    def destroy(self) -> None:
+        if self.handle:
+            self.lib.acDeviceDestroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+    # --- boxes ------------------------------------------------------------
+    def interior_box(self):
+        nx, ny, nz = self.n
+        g = abi.NGHOST
+        return i3(g, g, g), i3(g + nx, g + ny, g + nz)
+
+    def full_box(self):
+        nx, ny, nz = self.n
+        g = abi.NGHOST
+        return i3(0, 0, 0), i3(nx + 2 * g, ny + 2 * g, nz + 2 * g)
+
+    # --- data -------------------------------------------------------------
+    def load_mesh(self, host: abi.HostMesh, stream: int = 0) -> None:
+        _check(self.lib.acDeviceLoadMesh(self.handle, stream, host.cmesh), "acDeviceLoadMesh")
+
+    def store_mesh(self, host: abi.HostMesh, stream: int = 0) -> None:
+        _check(self.lib.acDeviceStoreMesh(self.handle, stream, C.byref(host.cmesh)),
+               "acDeviceStoreMesh")
+        self.synchronize(stream)
+
+    def load_double(self, handle: int, arr: np.ndarray, stream: int = 0) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        _check(self.lib.acDeviceLoadVertexBufferDouble(self.handle, stream, handle, a.ctypes.data),
+               "acDeviceLoadVertexBufferDouble")
+
+    def store_double(self, handle: int, stream: int = 0) -> np.ndarray:
+        nx, ny, nz = self.n
+        g = abi.NGHOST
+        out = np.empty((nz + 2 * g, ny + 2 * g, nx + 2 * g), dtype=np.float64)
+        _check(self.lib.acDeviceStoreVertexBufferDouble(self.handle, stream, handle,
+                                                         out.ctypes.data),
+               "acDeviceStoreVertexBufferDouble")
+        return out
+
+    def set_vertex_buffer(self, handle: int, value: float, stream: int = 0) -> None:
+        _check(self.lib.acDeviceSetVertexBuffer(self.handle, stream, handle, value),
+               "acDeviceSetVertexBuffer")
+
+    # --- uniforms ---------------------------------------------------------
+    def load_scalar_uniform(self, param: int, value: float, stream: int = 0) -> None:
+        _check(self.lib.acDeviceLoadScalarUniform(self.handle, stream, param, value),
+               "acDeviceLoadScalarUniform")
+
+    def load_mesh_info(self, info) -> None:
+        _check(self.lib.acDeviceLoadMeshInfo(self.handle, info), "acDeviceLoadMeshInfo")
+
+    # --- hot path ---------------------------------------------------------
+    def integrate_substep(self, step: int, dt: float, start=None, end=None, stream: int = 0) -> None:
+        if start is None:
+            start, end = self.interior_box()
+        _check(self.lib.acDeviceIntegrateSubstep(self.handle, stream, step, start, end, dt),
+               "acDeviceIntegrateSubstep")
+
+    def periodic_boundconds(self, stream: int = 0, start=None, end=None) -> None:
+        if start is None:
+            start, end = self.full_box()
+        _check(self.lib.acDevicePeriodicBoundconds(self.handle, stream, start, end),
+               "acDevicePeriodicBoundconds")
+
+    def swap_buffers(self) -> None:
+        _check(self.lib.acDeviceSwapBuffers(self.handle), "acDeviceSwapBuffers")
+
+    def integrate_step(self, dt: float, stream: int = 0) -> None:
+        _check(self.lib.acDeviceIntegrateStep(self.handle, stream, dt), "acDeviceIntegrateStep")
+
+    def integrate_steps(self, dt: float, n: int, stream: int = 0) -> None:
+        _check(self.lib.acDeviceIntegrateSteps(self.handle, stream, dt, n),
+               "acDeviceIntegrateSteps")
+
+    def set_forcing(self, enabled: bool) -> None:
+        _check(self.lib.acDeviceSetForcing(self.handle, int(bool(enabled))), "acDeviceSetForcing")
+
+    # --- reductions (device layer: RMS/RMS_EXP are raw sums) --------------
+    def reduce_scal(self, rtype: int, handle: int, stream: int = 0) -> float:
+        r = self.prec.real()
+        _check(self.lib.acDeviceReduceScal(self.handle, stream, rtype, handle, C.byref(r)),
+               "acDeviceReduceScal")
+        return float(r.value)
+
+    def reduce_vec(self, rtype: int, a: int, b: int, c: int, stream: int = 0) -> float:
+        r = self.prec.real()
+        _check(self.lib.acDeviceReduceVec(self.handle, stream, rtype, a, b, c, C.byref(r)),
+               "acDeviceReduceVec")
+        return float(r.value)
+
+    def reduce_scal_double(self, rtype: int, handle: int, stream: int = 0) -> float:
+        r = C.c_double()
+        _check(self.lib.acDeviceReduceScalDouble(self.handle, stream, rtype, handle, C.byref(r)),
+               "acDeviceReduceScalDouble")
+        return r.value
+
+    def reduce_vec_double(self, rtype: int, a: int, b: int, c: int, stream: int = 0) -> float:
+        r = C.c_double()
+        _check(self.lib.acDeviceReduceVecDouble(self.handle, stream, rtype, a, b, c, C.byref(r)),
+               "acDeviceReduceVecDouble")
+        return r.value
+
+    # --- plumbing -----------------------------------------------------------
+    def synchronize(self, stream: int = abi.STREAM_ALL) -> None:
+        _check(self.lib.acDeviceSynchronizeStream(self.handle, stream), "acDeviceSynchronizeStream")
+
+    def status(self) -> int:
+        s = C.c_uint()
+        _check(self.lib.acDeviceGetStatus(self.handle, C.byref(s)), "acDeviceGetStatus")
+        return s.value
+
+    def cuda_stream(self, stream: int = 0) -> int:
+        p = C.c_void_p()
+        _check(self.lib.acDeviceGetCudaStream(self.handle, stream, C.byref(p)),
+               "acDeviceGetCudaStream")
+        return p.value or 0
+
+    def launch_count(self) -> int:
+        c = C.c_ulonglong()
+        _check(self.lib.acDeviceGetLaunchCount(self.handle, C.byref(c)), "acDeviceGetLaunchCount")
+        return c.value
+
+    def set_solve_config(self, cfg: int) -> None:
+        _check(self.lib.acDeviceSetSolveConfig(self.handle, cfg), "acDeviceSetSolveConfig")
+
+    def solve_config(self) -> tuple[int, int, str]:
+        c, n = C.c_int(), C.c_int()
+        _check(self.lib.acDeviceGetSolveConfig(self.handle, C.byref(c), C.byref(n)),
+               "acDeviceGetSolveConfig")
+        return c.value, n.value, self.lib.acSolveConfigName(c.value).decode()
+
+    def auto_optimize(self) -> None:
+        _check(self.lib.acDeviceAutoOptimize(self.handle), "acDeviceAutoOptimize")
+
+    def memory_footprint(self) -> int:
+        b = C.c_size_t()
+        _check(self.lib.acDeviceGetMemoryFootprint(self.handle, C.byref(b)),
+               "acDeviceGetMemoryFootprint")
+        return b.value

@@ -1,0 +1,81 @@
+/*
+ * astaroth_b200.h -- entry points this library adds next to the reference
+ * interface. None of them has a counterpart in the reference's astaroth.h;
+ * existing callers never need them. All are exported with C linkage from the
+ * same library as astaroth.h and take plain pointers and sizes.
+ */
+#pragma once
+#include "astaroth.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status and plumbing ------------------------------------------------ */
+
+/* Sticky status word of the device: 0 when every kernel so far completed
+ * normally; bit 0 = a bounded wait on a TMA barrier timed out. Reading
+ * synchronises the device. */
+AcResult acDeviceGetStatus(const Device device, unsigned* status);
+
+/* The CUDA stream (cudaStream_t) behind a Stream handle, so a caller can
+ * order its own work or CUDA events with the device's. */
+AcResult acDeviceGetCudaStream(const Device device, const Stream stream, void** cuda_stream);
+
+/* Number of kernels this device has launched since creation. */
+AcResult acDeviceGetLaunchCount(const Device device, unsigned long long* count);
+
+/* Tile configuration of the solve kernel: index into the compiled table,
+ * -1 for the built-in default. acDeviceAutoOptimize picks one by timing. */
+AcResult acDeviceSetSolveConfig(const Device device, const int config);
+AcResult acDeviceGetSolveConfig(const Device device, int* config, int* num_configs);
+
+/* Descriptive name of a solve configuration (tile and pipeline depth). */
+const char* acSolveConfigName(const int config);
+
+/* Bytes of device memory held by the device's field blocks. */
+AcResult acDeviceGetMemoryFootprint(const Device device, size_t* bytes);
+
+/* ---- whole steps -------------------------------------------------------- */
+
+/* One full RK3 step on `stream`: three times (periodic ghost fill of every
+ * field, substep over the whole interior, buffer swap) -- the single-device
+ * acNodeIntegrate sequence. Asynchronous. */
+AcResult acDeviceIntegrateStep(const Device device, const Stream stream, const AcReal dt);
+
+/* `num_steps` full steps replayed from one captured CUDA graph (the graph is
+ * built on first use and rebuilt when dt or the configuration changes).
+ * Asynchronous; the buffer roles after the call are as after num_steps calls
+ * of acDeviceIntegrateStep. */
+AcResult acDeviceIntegrateSteps(const Device device, const Stream stream, const AcReal dt,
+                                const int num_steps);
+
+/* Enables the helical forcing term at the last substep
+ * (acc/mhd_solver/stencil_kernel.ac:611-648,713-717; off in the reference's
+ * shipped module). Its parameters are the AC_forcing_* / AC_k_force* /
+ * AC_ff_hel_* / AC_kaver uniforms. */
+AcResult acDeviceSetForcing(const Device device, const int enabled);
+
+/* ---- double-precision views (useful in every build; exact in dp) --------- */
+
+/* Loads / stores one whole field (mx*my*mz values, reference index order)
+ * from / to a double array. In the mixed build the double is split into the
+ * (hi, lo) float pair on load and recombined on store, so the state round
+ * trips at ~48-bit precision. */
+AcResult acDeviceLoadVertexBufferDouble(const Device device, const Stream stream,
+                                        const VertexBufferHandle handle, const double* src);
+AcResult acDeviceStoreVertexBufferDouble(const Device device, const Stream stream,
+                                         const VertexBufferHandle handle, double* dst);
+
+/* Reductions returning the FP64 accumulator (raw sums for RMS/RMS_EXP). */
+AcResult acDeviceReduceScalDouble(const Device device, const Stream stream,
+                                  const ReductionType rtype, const VertexBufferHandle handle,
+                                  double* result);
+AcResult acDeviceReduceVecDouble(const Device device, const Stream stream,
+                                 const ReductionType rtype, const VertexBufferHandle a,
+                                 const VertexBufferHandle b, const VertexBufferHandle c,
+                                 double* result);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif

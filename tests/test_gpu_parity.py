@@ -1,0 +1,362 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Tolerances (normwise per field: max|cand - model| / max|model| over the interior):
+  FP32  <= 1e-5     FP64 <= 1e-12     (vs the long-double oracle)
+  mixed <= 1e-5 vs the oracle; its distance to the FP64 GPU result is reported
+Load/store, ghost fill, sub-box updates, graph replay and tile choice are
+checked bit-exactly. Full-size behaviour is checked through size-independent
+properties (periodic-shift equivariance, reductions of a stored mesh).
+"""
+import ctypes as C
+import math
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from astaroth_b200 import Device, abi, init
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+FLAVOURS = ("sp", "dp", "mixed")
+TOL = {"sp": 1e-5, "dp": 1e-12, "mixed": 1e-5}
+PHYS = dict(gamma=5.0 / 3.0, nu_visc=5e-3, eta=5e-3, cs_sound=1.0, cp_sound=1.0)
+
+
+def workload_info(prec, nx, ny=None, nz=None, **kw):
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    p = dict(PHYS)
+    p.update(kw)
+    return abi.make_info(prec, nx, ny, nz, dsx=2 * math.pi / nx, dsy=2 * math.pi / ny,
+                         dsz=2 * math.pi / nz, **p)
+
+
+def new_device(flavour, info):
+    return Device(flavour, info)
+
+
+def run_gpu(flavour, fields, info, dt, steps, graph=False):
+    prec = abi.PRECISIONS[flavour]
+    host = abi.HostMesh(prec, info, [f.copy() for f in fields])
+    with new_device(flavour, info) as dev:
+        dev.load_mesh(host)
+        if graph:
+            dev.integrate_steps(dt, steps)
+        else:
+            for _ in range(steps):
+                dev.integrate_step(dt)
+        dev.periodic_boundconds()
+        dev.synchronize()
+        assert dev.status() == 0
+        out = [dev.store_double(w) for w in range(8)]
+    return out
+
+
+def interior(a):
+    g = abi.NGHOST
+    return a[g:-g, g:-g, g:-g]
+
+
+@pytest.mark.parametrize("flavour", FLAVOURS)
+def test_load_store_roundtrip(flavour):
+    prec = abi.PRECISIONS[flavour]
+    nx, ny, nz = 37, 29, 23
+    info = abi.make_info(prec, nx, ny, nz)
+    rng = np.random.default_rng(1)
+    fields = [rng.standard_normal((nz + 6, ny + 6, nx + 6)).astype(prec.np_dtype) for _ in range(8)]
+    host = abi.HostMesh(prec, info, fields)
+    back = abi.HostMesh(prec, info)
+    with new_device(flavour, info) as dev:
+        dev.load_mesh(host)
+        dev.store_mesh(back)
+        for w in range(8):
+            assert np.array_equal(back.fields[w], fields[w])
+        # a flat sub-range that starts and ends mid-row
+        part = abi.HostMesh(prec, info)
+        start, count = 1234, 5 * (nx + 6) + 17
+        k, rem = divmod(start, (nx + 6) * (ny + 6))
+        j, i = divmod(rem, nx + 6)
+        off = abi.int3(i, j, k)
+        rc = dev.lib.acDeviceStoreVertexBufferWithOffset(dev.handle, 0, 3, off, off, count,
+                                                         C.byref(part.cmesh))
+        assert rc == 0
+        dev.synchronize()
+        flat = part.fields[3].reshape(-1)
+        assert np.array_equal(flat[start:start + count], fields[3].reshape(-1)[start:start + count])
+
+
+@pytest.mark.parametrize("flavour", FLAVOURS)
+def test_periodic_boundconds_exact(flavour):
+    prec = abi.PRECISIONS[flavour]
+    nx, ny, nz = 21, 18, 13
+    info = abi.make_info(prec, nx, ny, nz)
+    rng = np.random.default_rng(2)
+    inter = [rng.standard_normal((nz, ny, nx)).astype(prec.np_dtype) for _ in range(8)]
+    fields = [np.zeros((nz + 6, ny + 6, nx + 6), prec.np_dtype) for _ in range(8)]
+    for f, v in zip(fields, inter):
+        f[3:-3, 3:-3, 3:-3] = v
+    host = abi.HostMesh(prec, info, fields)
+    back = abi.HostMesh(prec, info)
+    with new_device(flavour, info) as dev:
+        dev.load_mesh(host)
+        dev.periodic_boundconds()
+        dev.store_mesh(back)
+        for w in range(8):
+            assert np.array_equal(back.fields[w], init.wrap_ghosts(inter[w]))
+        # a sub-box fill touches only ghost vertices inside the box
+        dev.load_mesh(host)
+        s, e = abi.int3(0, 2, 1), abi.int3(nx + 6, 9, nz + 6)
+        assert dev.lib.acDevicePeriodicBoundcondStep(dev.handle, 0, 5, s, e) == 0
+        dev.store_mesh(back)
+        want = fields[5].copy()
+        full = init.wrap_ghosts(inter[5])
+        want[1:, 2:9, :] = full[1:, 2:9, :]
+        assert np.array_equal(back.fields[5], want)
+        assert np.array_equal(back.fields[4], fields[4])
+
+
+@pytest.fixture(scope="module")
+def oracle_64():
+    """Config 1: 64^3, 1e-3 noise (seed 1), dt = 1e-3, 10 steps, long double."""
+    n, steps, dt = 64, 10, 1e-3
+    info = workload_info(abi.DP, n)
+    fields = init.workload_fields(n, n, n, np.float32, seed=1, amplitude=1e-3)
+    om = O.OracleMesh("f80", fields, n, n, n)
+    om.step(O.params_from(info), float(np.float32(dt)), steps)
+    om.periodic()
+    return fields, om
+
+
+@pytest.mark.parametrize("flavour", FLAVOURS)
+def test_config1_64cube_10_steps_vs_oracle(flavour, oracle_64):
+    fields, om = oracle_64
+    prec = abi.PRECISIONS[flavour]
+    n, steps, dt = 64, 10, float(np.float32(1e-3))
+    info = workload_info(prec, n)
+    out = run_gpu(flavour, [f.astype(prec.np_dtype) for f in fields], info, dt, steps)
+    errs = [O.normwise_error(interior(out[w]), om.interior(w)) for w in range(8)]
+    print(flavour, ["%.2e" % e for e in errs])
+    assert max(errs) <= TOL[flavour], errs
+
+
+@pytest.mark.parametrize("flavour", FLAVOURS)
+def test_ragged_mesh_vs_oracle(flavour):
+    """Sizes that are not multiples of any tile, anisotropic spacing, larger amplitude."""
+    prec = abi.PRECISIONS[flavour]
+    nx, ny, nz, steps = 37, 29, 23, 2
+    info = abi.make_info(prec, nx, ny, nz, dsx=0.21, dsy=0.17, dsz=0.25, **PHYS)
+    fields = init.workload_fields(nx, ny, nz, prec.np_dtype, seed=11, amplitude=0.05,
+                                  velocity_mode=0.1)
+    dt = float(prec.np_dtype(2e-3))
+    out = run_gpu(flavour, fields, info, dt, steps)
+    om = O.OracleMesh("f80", fields, nx, ny, nz)
+    om.step(O.params_from(info), dt, steps)
+    errs = [O.normwise_error(interior(out[w]), om.interior(w)) for w in range(8)]
+    assert max(errs) <= TOL[flavour], errs
+
+
+@pytest.mark.parametrize("flavour", FLAVOURS)
+def test_reductions_vs_oracle(flavour):
+    prec = abi.PRECISIONS[flavour]
+    nx, ny, nz = 40, 33, 26
+    info = abi.make_info(prec, nx, ny, nz)
+    fields = init.workload_fields(nx, ny, nz, prec.np_dtype, seed=4, amplitude=0.3)
+    host = abi.HostMesh(prec, info, fields)
+    om = O.OracleMesh("f80", fields, nx, ny, nz)
+    with new_device(flavour, info) as dev:
+        dev.load_mesh(host)
+        for rt in (abi.RTYPE_MAX, abi.RTYPE_MIN, abi.RTYPE_RMS, abi.RTYPE_RMS_EXP, abi.RTYPE_SUM):
+            for w in (0, 3, 7):
+                got = dev.reduce_scal_double(rt, w)
+                want = om.reduce(rt, [w], normalise=False)  # device layer: raw sums
+                assert got == pytest.approx(want, rel=1e-12, abs=1e-12), (rt, w)
+            got = dev.reduce_vec_double(rt, 1, 2, 3)
+            want = om.reduce(rt, [1, 2, 3], normalise=False)
+            assert got == pytest.approx(want, rel=1e-12, abs=1e-12), rt
+            # the AcReal-returning entry points round the same accumulator
+            assert dev.reduce_scal(rt, 3) == pytest.approx(dev.reduce_scal_double(rt, 3),
+                                                           rel=1e-7 if prec.np_dtype == np.float32 else 1e-15)
+        # unsupported types fail instead of returning garbage
+        with pytest.raises(Exception):
+            dev.reduce_scal(abi.RTYPE_ALFVEN_MAX, 0)
+
+
+def test_node_reductions_are_normalised():
+    prec = abi.SP
+    n = 24
+    info = abi.make_info(prec, n)
+    fields = init.workload_fields(n, n, n, np.float32, seed=9, amplitude=0.2)
+    host = abi.HostMesh(prec, info, fields)
+    from astaroth_b200 import library
+
+    lib = library.load("sp")
+    node = C.c_void_p()
+    assert lib.acNodeCreate(0, info, C.byref(node)) == 0
+    try:
+        assert lib.acNodeLoadMesh(node, 0, host.cmesh) == 0
+        om = O.OracleMesh("f80", fields, n, n, n)
+        r = C.c_float()
+        assert lib.acNodeReduceScal(node, 0, abi.RTYPE_RMS, 2, C.byref(r)) == 0
+        assert r.value == pytest.approx(om.reduce(abi.RTYPE_RMS, [2], normalise=True), rel=1e-6)
+        assert lib.acNodeReduceVec(node, 0, abi.RTYPE_RMS_EXP, 1, 2, 3, C.byref(r)) == 0
+        assert r.value == pytest.approx(om.reduce(abi.RTYPE_RMS_EXP, [1, 2, 3], normalise=True),
+                                        rel=1e-6)
+    finally:
+        lib.acNodeDestroy(node)
+
+
+@pytest.mark.parametrize("flavour", ["sp", "dp"])
+def test_subbox_substep_matches_full(flavour):
+    prec = abi.PRECISIONS[flavour]
+    n = 40
+    info = workload_info(prec, n)
+    fields = init.workload_fields(n, n, n, prec.np_dtype, seed=5, amplitude=0.05)
+    host = abi.HostMesh(prec, info, fields)
+    dt = 1e-3
+    with new_device(flavour, info) as dev:
+        dev.load_mesh(host)
+        dev.periodic_boundconds()
+        dev.integrate_substep(0, dt)
+        dev.swap_buffers()
+        full = [dev.store_double(w) for w in range(8)]
+    with new_device(flavour, info) as dev:
+        dev.load_mesh(host)
+        dev.swap_buffers()  # out := the initial state, to see what is left untouched
+        dev.load_mesh(host)
+        dev.periodic_boundconds()
+        # the same substep over a box whose x start is not tile aligned
+        s, e = abi.int3(6, 4, 9), abi.int3(40, 31, 22)
+        dev.integrate_substep(0, dt, s, e)
+        dev.swap_buffers()
+        part = [dev.store_double(w) for w in range(8)]
+    for w in range(8):
+        box = (slice(9, 22), slice(4, 31), slice(6, 40))
+        assert np.array_equal(part[w][box], full[w][box])
+        mask = np.ones_like(part[w], dtype=bool)
+        mask[box] = False
+        assert np.array_equal(part[w][mask], fields[w].astype(np.float64)[mask])
+
+
+@pytest.mark.parametrize("flavour", FLAVOURS)
+def test_graph_replay_and_tile_configs_bitwise(flavour):
+    prec = abi.PRECISIONS[flavour]
+    n = 48
+    info = workload_info(prec, n)
+    fields = init.workload_fields(n, n, n, prec.np_dtype, seed=6, amplitude=0.05)
+    ref = run_gpu(flavour, fields, info, 1e-3, 3, graph=False)
+    got = run_gpu(flavour, fields, info, 1e-3, 3, graph=True)
+    for w in range(8):
+        assert np.array_equal(ref[w], got[w])
+    host = abi.HostMesh(prec, info, fields)
+    with new_device(flavour, info) as dev:
+        _, ncfg, _ = dev.solve_config()
+        for c in range(ncfg):
+            dev.set_solve_config(c)
+            dev.load_mesh(host)
+            for _ in range(3):
+                dev.integrate_step(1e-3)
+            dev.periodic_boundconds()
+            for w in range(8):
+                assert np.array_equal(dev.store_double(w), ref[w]), (c, w)
+
+
+def test_legacy_interface_matches_device_path():
+    prec = abi.SP
+    n = 32
+    info = workload_info(prec, n)
+    fields = init.workload_fields(n, n, n, np.float32, seed=8, amplitude=0.01)
+    host = abi.HostMesh(prec, info, [f.copy() for f in fields])
+    from astaroth_b200 import library
+
+    lib = library.load("sp")
+    assert lib.acInit(info) == 0
+    try:
+        assert lib.acLoad(host.cmesh) == 0
+        for _ in range(2):
+            assert lib.acIntegrate(np.float32(1e-3)) == 0
+        assert lib.acBoundcondStep() == 0
+        out = abi.HostMesh(prec, info)
+        assert lib.acStore(C.byref(out.cmesh)) == 0
+        umax = lib.acReduceVec(abi.RTYPE_MAX, 1, 2, 3)
+    finally:
+        lib.acQuit()
+    ref = run_gpu("sp", fields, info, float(np.float32(1e-3)), 2)
+    for w in range(8):
+        assert np.array_equal(out.fields[w].astype(np.float64), ref[w])
+    assert umax == pytest.approx(np.max(np.sqrt(sum(interior(ref[c]) ** 2 for c in (1, 2, 3)))),
+                                 rel=1e-6)
+
+
+@pytest.mark.parametrize("flavour", ["sp", "dp"])
+def test_forcing_vs_oracle(flavour):
+    prec = abi.PRECISIONS[flavour]
+    n, steps = 24, 2
+    kf, ffr, ffi = (1.0, -2.0, 1.0), (0.1, 0.2, -0.3), (0.3, -0.1, 0.2)
+    extra = dict(forcing_magnitude=0.05, forcing_phase=0.7, kaver=1.0, k_forcex=kf[0],
+                 k_forcey=kf[1], k_forcez=kf[2], ff_hel_rex=ffr[0], ff_hel_rey=ffr[1],
+                 ff_hel_rez=ffr[2], ff_hel_imx=ffi[0], ff_hel_imy=ffi[1], ff_hel_imz=ffi[2])
+    info = workload_info(prec, n, **extra)
+    fields = init.workload_fields(n, n, n, prec.np_dtype, seed=12, amplitude=1e-3)
+    host = abi.HostMesh(prec, info, [f.copy() for f in fields])
+    dt = float(prec.np_dtype(1e-3))
+    with new_device(flavour, info) as dev:
+        dev.set_forcing(True)
+        dev.load_mesh(host)
+        for _ in range(steps):
+            dev.integrate_step(dt)
+        out = [dev.store_double(w) for w in range(8)]
+    p = O.params_from(info, forcing=1, forcing_magnitude=abi.get_real(info, "forcing_magnitude"),
+                      forcing_phase=abi.get_real(info, "forcing_phase"), kaver=1.0,
+                      k_force=[abi.get_real(info, k) for k in ("k_forcex", "k_forcey", "k_forcez")],
+                      ff_re=[abi.get_real(info, k) for k in ("ff_hel_rex", "ff_hel_rey", "ff_hel_rez")],
+                      ff_im=[abi.get_real(info, k) for k in ("ff_hel_imx", "ff_hel_imy", "ff_hel_imz")])
+    om = O.OracleMesh("f80", fields, n, n, n)
+    om.step(p, dt, steps)
+    errs = [O.normwise_error(interior(out[w]), om.interior(w)) for w in range(8)]
+    assert max(errs) <= TOL[flavour], errs
+
+
+def test_mixed_tracks_fp64():
+    """The mixed state stays close to the FP64 GPU path (64^3, 10 steps)."""
+    n, steps, dt = 64, 10, float(np.float32(1e-3))
+    fields = init.workload_fields(n, n, n, np.float32, seed=1, amplitude=1e-3, velocity_mode=0.1)
+    d = run_gpu("dp", [f.astype(np.float64) for f in fields], workload_info(abi.DP, n), dt, steps)
+    m = run_gpu("mixed", fields, workload_info(abi.MIXED, n), dt, steps)
+    s = run_gpu("sp", fields, workload_info(abi.SP, n), dt, steps)
+    em = [O.normwise_error(interior(m[w]), interior(d[w])) for w in range(8)]
+    es = [O.normwise_error(interior(s[w]), interior(d[w])) for w in range(8)]
+    print("mixed vs dp", ["%.2e" % e for e in em])
+    print("sp    vs dp", ["%.2e" % e for e in es])
+    assert max(em) <= 1e-5
+
+
+@pytest.mark.parametrize("flavour", ["sp", "mixed"])
+def test_shift_equivariance_256(flavour):
+    """Full-size property: a periodic shift of the initial state shifts the
+    result exactly (every vertex runs the same arithmetic)."""
+    prec = abi.PRECISIONS[flavour]
+    n = 256
+    info = workload_info(prec, n)
+    fields = init.workload_fields(n, n, n, prec.np_dtype, seed=3, amplitude=1e-3, velocity_mode=0.1)
+    shift = (5, -37, 101)
+    shifted = [init.wrap_ghosts(np.roll(f[3:-3, 3:-3, 3:-3], shift, axis=(0, 1, 2)))
+               for f in fields]
+    a = run_gpu(flavour, fields, info, 1e-3, 1)
+    b = run_gpu(flavour, shifted, info, 1e-3, 1)
+    for w in range(8):
+        assert np.array_equal(np.roll(interior(a[w]), shift, axis=(0, 1, 2)), interior(b[w]))
+
+
+def test_reference_ctest_sample_runs(tmp_path):
+    exe = os.path.join(abi.REPO, "oracle", "_ref", "ctest_sp")
+    if not os.path.exists(exe):
+        pytest.skip("ctest binary not built (needs the reference sources at build time)")
+    cfg = tmp_path / "astaroth.conf"
+    lines = [f"{k} = {v}" for k, v in abi.DEFAULT_CONFIG.items() if k != "AC_bin_save_t"]
+    cfg.write_text("\n".join(lines) + "\n")
+    r = subprocess.run([exe], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "ctest complete." in r.stdout
+    assert "FAIL" not in r.stdout
