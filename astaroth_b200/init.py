@@ -48,6 +48,65 @@ def noise_interior(seed: int, field: int, nx: int, ny: int, nz: int, amplitude: 
     return (amplitude * uniform_pm1(seed, field, idx)).reshape(k1 - k0, ny, nx)
 
 
+def noise_interior_torch(seed: int, field: int, nx: int, ny: int, nz: int, amplitude: float,
+                         device="cuda"):
+    """Same values as noise_interior (bit for bit), generated with torch on
+    `device`; int64 arithmetic wraps like uint64, logical shifts are masked."""
+    import torch
+
+    def lsr(x, s):
+        return (x >> s) & ((1 << (64 - s)) - 1)
+
+    def as_i64(u: int) -> int:
+        return u - (1 << 64) if u >= (1 << 63) else u
+
+    m1, m2, gold = as_i64(0xBF58476D1CE4E5B9), as_i64(0x94D049BB133111EB), as_i64(0x9E3779B97F4A7C15)
+    mul = as_i64(0x100000001B3)
+    key = as_i64(((seed & 0xFFFFFFFF) << 32) | ((field & 0xFF) << 24))
+    out = torch.empty((nz, ny, nx), dtype=torch.float64, device=device)
+    plane = nx * ny
+    chunk = max(1, (1 << 26) // plane)
+    for k0 in range(0, nz, chunk):
+        k1 = min(nz, k0 + chunk)
+        idx = torch.arange(k0 * plane, k1 * plane, dtype=torch.int64, device=device)
+        z = (idx * mul) ^ key
+        z = z + gold
+        z = (z ^ lsr(z, 30)) * m1
+        z = (z ^ lsr(z, 27)) * m2
+        z = z ^ lsr(z, 31)
+        u = lsr(z, 11).to(torch.float64) * (1.0 / 9007199254740992.0)
+        out[k0:k1] = (amplitude * (2.0 * u - 1.0)).reshape(k1 - k0, ny, nx)
+    return out
+
+
+def workload_fields_torch(nx: int, ny: int, nz: int, dtype, seed: int = 1,
+                          amplitude: float = 1e-3, velocity_mode: float = 0.0, device="cuda"):
+    """Torch twin of workload_fields: returns eight (nz+6, ny+6, nx+6) tensors of
+    `dtype` (a torch dtype) with periodic ghosts, equal to the numpy version."""
+    import torch
+
+    out = []
+    for w in range(NUM_VTXBUF_HANDLES):
+        f = noise_interior_torch(seed, w, nx, ny, nz, amplitude, device)
+        if velocity_mode and w in (1, 2, 3):
+            axis, n = {1: ("y", ny), 2: ("z", nz), 3: ("x", nx)}[w]
+            s = velocity_mode * torch.sin(
+                2.0 * (2.0 * math.pi / n) * torch.arange(n, dtype=torch.float64, device=device))
+            if axis == "x":
+                f += s[None, None, :]
+            elif axis == "y":
+                f += s[None, :, None]
+            else:
+                f += s[:, None, None]
+        g = f.to(dtype)
+        del f
+        g = torch.cat([g[-NGHOST:], g, g[:NGHOST]], dim=0)
+        g = torch.cat([g[:, -NGHOST:], g, g[:, :NGHOST]], dim=1)
+        g = torch.cat([g[:, :, -NGHOST:], g, g[:, :, :NGHOST]], dim=2)
+        out.append(g.contiguous())
+    return out
+
+
 def wrap_ghosts(interior: np.ndarray) -> np.ndarray:
     """Pad an interior (nz, ny, nx) array with NGHOST periodic ghost cells per side;
     equal to applying the reference's periodic boundary conditions."""

@@ -1,0 +1,479 @@
+#!/usr/bin/env python
+"""RK3 cell-updates/s of the single-device MHD solver, 512^3 workload.
+
+Workload (the headline configuration): 512^3 mesh, eight fields
+(lnrho, ux, uy, uz, ax, ay, az, entropy), seeded 1e-3 * U(-1,1) noise plus the
+k = 2 velocity mode u = 0.1 (sin 2y, sin 2z, sin 2x), dx = 2 pi / 512,
+nu = eta = 5e-3, cs = 1, gamma = 5/3, cp = 1, dt = 1e-3, periodic.
+The measured arm is the mixed-precision library (FP32 stencils and right-hand
+sides, compensated (hi, lo) FP32 state, FP64 reductions); the plain FP64 and
+FP32 libraries run the same steps beside it for the comparison and the error.
+
+One step = three substeps, each a periodic ghost fill of all fields plus one
+fused solve launch, all through the C ABI (acDevicePeriodicBoundconds,
+acDeviceIntegrateSubstep, acDeviceSwapBuffers). Inputs are larger than L2
+(8.9 GB of state per block), so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU runs are replicas (the path has no exchange step on one device):
+every rank advances its own mesh; value = all ranks' cell updates / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "RK3 cell-updates/s at 512^3 (mixed precision; FP64 and FP32 alongside)"
+UNIT = "cell-updates/s"
+N_DEFAULT = 512
+DT = 1e-3
+PHYS = dict(gamma=5.0 / 3.0, nu_visc=5e-3, eta=5e-3, cs_sound=1.0, cp_sound=1.0)
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=N_DEFAULT, help="mesh size (default 512)")
+    ap.add_argument("--no-variants", action="store_true", help="skip the FP64/FP32 side runs")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------
+# ranks
+# ---------------------------------------------------------------------------
+class Ranks:
+    def __init__(self, gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local))
+            self.dist = dist
+
+    def barrier(self):
+        import torch
+
+        torch.cuda.synchronize()
+        if self.dist:
+            self.dist.barrier()
+        torch.cuda.synchronize()
+
+    def max(self, x: float) -> float:
+        if not self.dist:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            text, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            text, _ = self.proc.communicate()
+        rows = [r for r in csv.reader(io.StringIO(text)) if len(r) >= 9]
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                power.append(float(r[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def workload_info(prec, n: int):
+    from astaroth_b200 import abi
+
+    ds = 2.0 * math.pi / n
+    return abi.make_info(prec, n, n, n, dsx=ds, dsy=ds, dsz=ds, **PHYS)
+
+
+def host_mesh(flavour: str, n: int, pinned: bool = True):
+    """The seeded initial state as a pinned host AcMesh of the flavour's AcReal.
+    Values are generated on the GPU (bit-identical to the numpy generator),
+    rounded to float32 once; the FP64 library gets the same float32 values."""
+    import torch
+
+    from astaroth_b200 import abi, init
+
+    prec = abi.PRECISIONS[flavour]
+    info = workload_info(prec, n)
+    tdt = torch.float64 if prec.double else torch.float32
+    host = abi.HostMesh(prec, info, pinned=pinned)
+    gen = init.workload_fields_torch(n, n, n, torch.float32, seed=1, amplitude=1e-3,
+                                     velocity_mode=0.1, device="cuda")
+    for w, g in enumerate(gen):
+        host.fields[w][...] = g.to(tdt).cpu().numpy()
+    del gen
+    torch.cuda.empty_cache()
+    return host
+
+
+def alg_bytes_per_step(flavour: str, n: int) -> int:
+    """Algorithmic HBM bytes of the three solve launches of one step: every
+    array touched once per substep (s = 0: read in, write out; s = 1, 2: read
+    in, read out, write out), eight fields. FP32 4 B, FP64 8 B, mixed 8 B
+    (float hi + float lo) per value."""
+    w = {"sp": 4, "dp": 8, "mixed": 8}[flavour]
+    return 8 * w * (2 + 3 + 3) * n ** 3
+
+
+def timed_steps(dev, steps: int, warmup: int, ranks, sample_clocks=False, gpu_index=0):
+    """Runs warmup + steps RK3 steps through the C ABI; returns device-timed
+    figures (CUDA events on the device's stream, max over ranks)."""
+    import torch
+
+    st = torch.cuda.ExternalStream(dev.cuda_stream(0))
+    for _ in range(warmup):
+        for s in range(3):
+            dev.periodic_boundconds()
+            dev.integrate_substep(s, DT)
+            dev.swap_buffers()
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    pairs = [[(ev(), ev()) for _ in range(3)] for _ in range(steps)]
+    e0, e1 = ev(), ev()
+    clocks = ClockSampler(gpu_index) if sample_clocks else None
+    ranks.barrier()
+    launches0 = dev.launch_count()
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    e0.record(st)
+    for k in range(steps):
+        for s in range(3):
+            dev.periodic_boundconds()
+            pairs[k][s][0].record(st)
+            dev.integrate_substep(s, DT)
+            pairs[k][s][1].record(st)
+            dev.swap_buffers()
+    e1.record(st)
+    e1.synchronize()
+    ranks.barrier()
+    clk = clocks.stop() if clocks else None
+    launches = dev.launch_count() - launches0
+    total_ms = ranks.max(e0.elapsed_time(e1))
+    solve_ms = [[a.elapsed_time(b) for a, b in row] for row in pairs]
+    solve_total = ranks.max(sum(sum(r) for r in solve_ms))
+    per_substep = [statistics.mean(r[s] for r in solve_ms) for s in range(3)]
+    return {"total_ms": total_ms, "ms_per_step": total_ms / steps,
+            "solve_ms_total": solve_total, "solve_ms_per_substep": per_substep,
+            "launches": launches, "clocks": clk}
+
+
+def field_errors(dev_a, dev_b, n: int) -> list[float]:
+    """Per-field normwise error max|a - b| / max|b| over the interior, from the
+    double views of the two devices' current states."""
+    import torch
+
+    g = 3
+    errs = []
+    for w in range(8):
+        a = torch.from_numpy(dev_a.store_double(w)).cuda()[g:-g, g:-g, g:-g]
+        b = torch.from_numpy(dev_b.store_double(w)).cuda()[g:-g, g:-g, g:-g]
+        den = float(b.abs().max())
+        errs.append(float((a - b).abs().max()) / den if den > 0 else float((a - b).abs().max()))
+        del a, b
+    torch.cuda.empty_cache()
+    return errs
+
+
+def e2e_run(flavour: str, host, steps: int, ranks) -> dict:
+    """The same steps end to end through the public C ABI with host buffers:
+    load the mesh from pinned host memory, per step one RK3 step
+    (acDeviceIntegrateStep) and one diagnostic reduction read back to the host
+    (max |u|, as a CFL check does), then store the mesh to pinned host memory."""
+    import torch
+
+    from astaroth_b200 import Device, abi
+
+    n = abi.dims(host.info)[0]
+    dev = Device(flavour, host.info, torch.cuda.current_device())
+    out = abi.HostMesh(host.prec, host.info, pinned=True)
+    dev.load_mesh(host)
+    dev.integrate_step(DT)  # warm the kernels and graph-free path
+    dev.synchronize()
+    ranks.barrier()
+    t0 = time.perf_counter()
+    dev.load_mesh(host)
+    umax = 0.0
+    for _ in range(steps):
+        dev.integrate_step(DT)
+        umax = dev.reduce_vec(abi.RTYPE_MAX, abi.VTXBUF_UUX, abi.VTXBUF_UUY, abi.VTXBUF_UUZ)
+    dev.store_mesh(out)
+    dev.synchronize()
+    t = ranks.max(time.perf_counter() - t0)
+    mesh_bytes = 8 * host.fields[0].nbytes
+    dev.destroy()
+    del out
+    return {"seconds": t, "cells_per_s": ranks.world * n ** 3 * steps / t,
+            "h2d_bytes_per_step": mesh_bytes / steps, "d2h_bytes_per_step": 8 + mesh_bytes / steps,
+            "umax": umax}
+
+
+def cpu_reference_sample(budget_s: float = 12.0, n: int = 64, max_steps: int | None = None,
+                         warmup: int = 0) -> dict:
+    """The reference's own host solver (src/utils/modelsolver.c acHostIntegrateStep,
+    built from its sources into oracle/_ref) on an n^3 sample of the same
+    physics; the oracle port (OpenMP) where that build is absent."""
+    sys.path.insert(0, os.path.join(HERE, "tests"))
+    import numpy as np
+
+    import oracle_lib as O
+    from astaroth_b200 import abi, init
+
+    info = workload_info(abi.SP, n)
+    fields = init.workload_fields(n, n, n, np.float32, seed=1, amplitude=1e-3, velocity_mode=0.1)
+    ref = O.ref_lib("sp")
+    if ref is not None:
+        hm = abi.HostMesh(abi.SP, info, fields)
+
+        def step():
+            ref.acHostIntegrateStep(hm.cmesh, abi.SP.real(DT))
+
+        kind, cores = "reference", 1
+        what = "reference src/utils/modelsolver.c acHostIntegrateStep (FP32), 1 thread"
+    else:
+        om = O.OracleMesh("f32", fields, n, n, n)
+        p = O.params_from(info)
+
+        def step():
+            om.step(p, float(np.float32(DT)))
+
+        kind, cores = "port", os.cpu_count() or 1
+        what = "oracle/mhd_oracle.c (FP32 restatement), OpenMP on all cores"
+    for _ in range(warmup):
+        step()
+    times = []
+    t_start = time.perf_counter()
+    while True:
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+        if max_steps is not None and len(times) >= max_steps:
+            break
+        if max_steps is None and time.perf_counter() - t_start >= budget_s:
+            break
+    tot = sum(times)
+    return {"value": n ** 3 * len(times) / tot, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{len(times)} RK3 steps of a {n}^3 mesh of the same physics; {what}",
+            "ms_per_step": 1e3 * tot / len(times), "steps": len(times)}
+
+
+def profile_traffic(name: str):
+    """Per-launch DRAM bytes of the dominant kernel from a committed ncu
+    summary (a line `traffic_bytes_per_launch: <value>`), else None."""
+    path = os.path.join(HERE, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+def measured_peak_hbm():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def config_block(n: int, world: int) -> dict:
+    return {"workload": f"MHD RK3, {n}^3, 8 fields, mixed precision (FP32 RHS, compensated FP32 "
+                        f"state, FP64 reductions); seeded 1e-3 noise + k=2 velocity mode 0.1",
+            "mesh": [n, n, n], "fields": 8, "dt": DT, "dx": "2*pi/n", "nu": 5e-3, "eta": 5e-3,
+            "cs": 1.0, "gamma": 5.0 / 3.0, "cp": 1.0,
+            "step": "3 x (periodic ghost fill + fused solve launch + swap) through the C ABI",
+            "l2": "inputs larger than L2 (8.9 GB per state block); no flush",
+            "parallelism": f"replicas x{world}" if world > 1 else "single device"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return  # the reference CPU arm runs on rank 0 only
+    r = cpu_reference_sample(n=64, max_steps=args.steps, warmup=args.warmup)
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": r["steps"], "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": config_block(args.n, 1),
+            "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+
+    from astaroth_b200 import Device, abi
+
+    ranks = Ranks(args.gpus)
+    gpu = ranks.local
+    torch.cuda.set_device(gpu)
+    n = args.n
+    host = host_mesh("mixed", n)
+    dev = Device("mixed", host.info, gpu)
+    dev.load_mesh(host)
+    res = timed_steps(dev, args.steps, args.warmup, ranks, sample_clocks=True, gpu_index=gpu)
+    cells = ranks.world * n ** 3 * args.steps
+    value = cells / (res["total_ms"] * 1e-3)
+
+    # roofline of the dominant kernel (the fused solve): algorithmic bytes per
+    # launch over the average launch time from the events around every launch
+    alg = alg_bytes_per_step("mixed", n)
+    achieved_gbs = alg * args.steps / (res["solve_ms_total"] * 1e-3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    traffic = profile_traffic("solve_mixed_512.md")
+
+    variants = {}
+    errors = None
+    if not args.no_variants:
+        # the same warmup + steps from the same float32 initial values
+        side = {}
+        for flav in ("dp", "sp"):
+            h = host_mesh(flav, n)
+            d = Device(flav, h.info, gpu)
+            d.load_mesh(h)
+            del h
+            r = timed_steps(d, args.steps, args.warmup, ranks)
+            variants[flav] = {
+                "value": ranks.world * n ** 3 * args.steps / (r["total_ms"] * 1e-3),
+                "ms_per_step": r["ms_per_step"],
+                "solve_ms_per_substep": r["solve_ms_per_substep"],
+                "solve_hbm_gbs_alg": alg_bytes_per_step(flav, n) * args.steps
+                / (r["solve_ms_total"] * 1e-3) / 1e9}
+            side[flav] = d
+        # per-field normwise error (interior) after warmup + steps steps
+        errors = {"metric": "max|x - x_fp64| / max|x_fp64| per field after "
+                            f"{args.warmup + args.steps} steps",
+                  "fields": list(abi.VTXBUFS),
+                  "mixed_vs_fp64": field_errors(dev, side["dp"], n),
+                  "fp32_vs_fp64": field_errors(side["sp"], side["dp"], n)}
+        for d in side.values():
+            d.destroy()
+        variants["speedup_mixed_over_fp64"] = value / variants["dp"]["value"]
+    dev.destroy()
+    del host
+    torch.cuda.empty_cache()
+
+    e2e = None
+    if not args.no_e2e:
+        h = host_mesh("mixed", n)
+        e = e2e_run("mixed", h, args.steps, ranks)
+        e2e = {"value": e["cells_per_s"], "unit": UNIT,
+               "h2d_bytes_per_step": e["h2d_bytes_per_step"],
+               "d2h_bytes_per_step": e["d2h_bytes_per_step"],
+               "includes": "mesh load from pinned host, per-step max|u| read back, mesh store"}
+        del h
+
+    cpu = None
+    if ranks.rank == 0 and not args.no_cpu:
+        c = cpu_reference_sample(budget_s=12.0)
+        cpu = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if ranks.rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 (compensated f32-pair state, f64 reductions)", "data": "synthetic",
+                "config": config_block(n, ranks.world),
+                "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak,
+                             "unit": "GB/s", "frac": achieved_gbs / peak,
+                             "traffic": traffic, "peak_source": peak_kind,
+                             "kernel": "solve_kernel (mixed)",
+                             "alg_bytes_per_cell_step": alg // n ** 3,
+                             "solve_ms_per_substep": res["solve_ms_per_substep"]},
+                "clocks": res["clocks"], "gpu_launches": res["launches"],
+                "e2e": e2e, "cpu_baseline": cpu, "variants": variants, "errors": errors}
+        print(json.dumps(line), flush=True)
+    ranks.close()
+
+
+def main(argv=None) -> None:
+    args = parse_args(argv)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
