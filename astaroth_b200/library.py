@@ -54,7 +54,7 @@ ASTAROTH_B200_H = [
     "acDeviceSetSolveConfig", "acDeviceGetSolveConfig", "acSolveConfigName",
     "acDeviceGetMemoryFootprint", "acDeviceIntegrateStep", "acDeviceIntegrateSteps",
     "acDeviceSetForcing", "acDeviceLoadVertexBufferDouble", "acDeviceStoreVertexBufferDouble",
-    "acDeviceReduceScalDouble", "acDeviceReduceVecDouble",
+    "acDeviceReduceScalDouble", "acDeviceReduceVecDouble", "acReduceScalNoAlloc",
 ]
 ALL_SYMBOLS = ASTAROTH_H + ASTAROTH_UTILS_H + ASTAROTH_B200_H
 
@@ -155,6 +155,7 @@ def _declare(lib: C.CDLL, prec: abi.Precision) -> None:
         "acDeviceStoreVertexBufferDouble": (res, [Dev, i, i, C.c_void_p]),
         "acDeviceReduceScalDouble": (res, [Dev, i, i, i, C.POINTER(C.c_double)]),
         "acDeviceReduceVecDouble": (res, [Dev, i, i, i, i, i, C.POINTER(C.c_double)]),
+        "acReduceScalNoAlloc": (res, [C.c_void_p, i, C.c_void_p, i, i, i, C.c_void_p]),
     }
     for name, (rt, args) in sig.items():
         fn = getattr(d, name)

@@ -76,6 +76,23 @@ AcResult acDeviceReduceVecDouble(const Device device, const Stream stream,
                                  const VertexBufferHandle b, const VertexBufferHandle c,
                                  double* result);
 
+/* ---- reduction without device allocation --------------------------------
+ * No counterpart in the reference. For callers that cannot call cudaMalloc
+ * (a framework that owns all device memory through its own pool, or a loop
+ * that must not pay cudaMalloc's implicit synchronisation): reduces the
+ * interior of a caller-owned device field and allocates nothing.
+ *   cuda_stream  cudaStream_t to launch on (asynchronous; no synchronisation)
+ *   field        device pointer, (nx+6)*(ny+6)*(nz+6) AcReal in the reference
+ *                index order i + j*mx + k*mx*my
+ *   result       device pointer to one double; receives the FP64 accumulator
+ *                (RMS and RMS_EXP as raw sums, like acDeviceReduceScal)
+ * Scratch lives in a fixed 128 KiB array of the library on each GPU, so
+ * meshes with ny*nz > 1,048,576 are rejected (AC_FAILURE), calls that overlap
+ * on the GPU race, and the first call on a device looks up the array's device
+ * address (make that first call before any stream capture). */
+AcResult acReduceScalNoAlloc(void* cuda_stream, const ReductionType rtype, const AcReal* field,
+                             const int nx, const int ny, const int nz, double* result);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
