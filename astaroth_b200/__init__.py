@@ -5,6 +5,6 @@ include/astaroth.h, astaroth_utils.h, astaroth_b200.h); this package holds its
 build script and a thin Python mirror of the reference's Device interface.
 """
 from . import abi  # noqa: F401
-from .device import AcError, Device  # noqa: F401
+from .device import AcError, Device, Ensemble  # noqa: F401
 
-__all__ = ["abi", "Device", "AcError"]
+__all__ = ["abi", "Device", "Ensemble", "AcError"]

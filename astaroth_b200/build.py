@@ -32,9 +32,9 @@ FLAVOURS = {
     "dp": ["-DAC_DOUBLE_PRECISION=1", "-DACB_MIXED=0"],
     "mixed": ["-DAC_DOUBLE_PRECISION=0", "-DACB_MIXED=1"],
 }
-CU_SOURCES = ["device.cu", "reduce_noalloc.cu"]
+CU_SOURCES = ["device.cu", "ensemble.cu", "reduce_noalloc.cu"]
 CXX_SOURCES = ["node.cc", "host_utils.cc", "host_model.cc"]
-HEADERS = ["common.cuh", "tma.cuh", "solve.cuh", "halo.cuh", "reduce.cuh"]
+HEADERS = ["common.cuh", "tma.cuh", "solve.cuh", "halo.cuh", "reduce.cuh", "internal.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

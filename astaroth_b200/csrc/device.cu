@@ -24,67 +24,29 @@
 #include "halo.cuh"
 #include "reduce.cuh"
 #include "solve.cuh"
+#include "internal.cuh"
 
-// ---------------------------------------------------------------------------
-// Solve configurations (tile width, tile height, ring depth)
-// ---------------------------------------------------------------------------
-#if AC_DOUBLE_PRECISION == 1
-using SolveCfg0 = TileCfg<32, 4, 8, 1>;
-using SolveCfg1 = TileCfg<16, 8, 8, 1>;
-using SolveCfg2 = TileCfg<32, 2, 10, 2>;
-#else
-using SolveCfg0 = TileCfg<32, 8, 9, 1>;
-using SolveCfg1 = TileCfg<32, 4, 10, 1>;
-using SolveCfg2 = TileCfg<64, 4, 8, 1>;
-#endif
+using namespace acb_host;
 
-typedef void (*SolveKernelFn)(const CUtensorMap, const SolveArgs<AcReal>);
-
-struct SolveConfig {
-    const char* name;
-    int TX, TY, NP, threads;
-    size_t smem;
-    SolveKernelFn kern[3];
-};
-
-template <class Cfg>
-static SolveConfig
-make_config(const char* name)
-{
-    SolveConfig c;
-    c.name    = name;
-    c.TX      = Cfg::TX;
-    c.TY      = Cfg::TY;
-    c.NP      = Cfg::NP;
-    c.threads = Cfg::THREADS;
-    c.smem    = Cfg::smem_bytes();
-    c.kern[0] = solve_kernel<Cfg, 0>;
-    c.kern[1] = solve_kernel<Cfg, 1>;
-    c.kern[2] = solve_kernel<Cfg, 2>;
-    return c;
-}
-
-static const SolveConfig*
-solve_configs(int* n)
+const SolveConfig*
+acb_host::solve_configs(int* n)
 {
 #if AC_DOUBLE_PRECISION == 1
     static const SolveConfig table[] = {
-        make_config<SolveCfg0>("tile32x4_ring8"),
-        make_config<SolveCfg1>("tile16x8_ring8"),
-        make_config<SolveCfg2>("tile32x2_ring10"),
+        make_solve_config<SolveCfg0, false>("tile32x4_ring8"),
+        make_solve_config<SolveCfg1, false>("tile16x8_ring8"),
+        make_solve_config<SolveCfg2, false>("tile32x2_ring10"),
     };
 #else
     static const SolveConfig table[] = {
-        make_config<SolveCfg0>("tile32x8_ring9"),
-        make_config<SolveCfg1>("tile32x4_ring10"),
-        make_config<SolveCfg2>("tile64x4_ring8"),
+        make_solve_config<SolveCfg0, false>("tile32x8_ring9"),
+        make_solve_config<SolveCfg1, false>("tile32x4_ring10"),
+        make_solve_config<SolveCfg2, false>("tile64x4_ring8"),
     };
 #endif
     *n = (int)(sizeof(table) / sizeof(table[0]));
     return table;
 }
-
-static const int kDefaultSolveConfig = 0;
 
 // ---------------------------------------------------------------------------
 // The device object
@@ -100,6 +62,10 @@ struct device_s {
     state_t* blk[2]; // the two field blocks; blk[cur] is `in`
     float* lo[2];    // mixed build: lo parts of the blocks
     int cur;
+    // ghost_ok[b]: block b's ghost zone holds the periodic images of its
+    // interior (set by a full-box fill of all fields; cleared by any write to
+    // the block). A fill of a block whose ghosts are already valid is skipped.
+    bool ghost_ok[2];
 
     CUtensorMap tmap[2];
     int tmap_cfg; // configuration the maps were encoded for (-1: none)
@@ -122,6 +88,8 @@ struct device_s {
     // whole-step graphs, one per starting buffer parity
     cudaGraphExec_t graph[2];
     unsigned long long graph_key[2];
+    unsigned long long graph_launches[2];
+    bool graph_ghost[2][2]; // ghost_ok of both blocks after a replay of graph[p]
 };
 
 // ---------------------------------------------------------------------------
@@ -161,16 +129,15 @@ get_encode_tiled()
     return fn;
 }
 
-// 4-D map (x, y, z, field) over one field block with a (TX+8, TY+6, 1, 8) box
-static AcResult
-encode_block_map(const Device d, int b, const SolveConfig& cfg, CUtensorMap* map)
+AcResult
+acb_host::encode_block_map(const Layout& L, const state_t* block, const SolveConfig& cfg,
+                           CUtensorMap* map)
 {
     PFN_encodeTiled_t enc = get_encode_tiled();
     if (!enc) {
         fprintf(stderr, "astaroth_b200: cuTensorMapEncodeTiled unavailable\n");
         return AC_FAILURE;
     }
-    const Layout& L          = d->L;
     const cuuint64_t esz     = sizeof(state_t);
     const cuuint64_t dim[4]  = {(cuuint64_t)L.mxp, (cuuint64_t)L.my, (cuuint64_t)L.mz, ACB_NF};
     const cuuint64_t str[3]  = {(cuuint64_t)L.mxp * esz, (cuuint64_t)L.plane * esz,
@@ -180,7 +147,7 @@ encode_block_map(const Device d, int b, const SolveConfig& cfg, CUtensorMap* map
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     const CUtensorMapDataType dt = sizeof(state_t) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
                                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    CUresult r = enc(map, dt, 4, (void*)d->blk[b], dim, str, box, estr,
+    CUresult r = enc(map, dt, 4, (void*)block, dim, str, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
@@ -198,9 +165,20 @@ ensure_maps(const Device d)
     int n;
     const SolveConfig* cfgs = solve_configs(&n);
     for (int b = 0; b < 2; ++b)
-        if (encode_block_map(d, b, cfgs[d->solve_cfg], &d->tmap[b]) != AC_SUCCESS)
+        if (encode_block_map(d->L, d->blk[b], cfgs[d->solve_cfg], &d->tmap[b]) != AC_SUCCESS)
             return AC_FAILURE;
     d->tmap_cfg = d->solve_cfg;
+    return AC_SUCCESS;
+}
+
+AcResult
+acb_host::prepare_table(const SolveConfig* cfgs, int n)
+{
+    for (int c = 0; c < n; ++c)
+        for (int st = 0; st < 3; ++st)
+            ACB_CUDA_CHECK(cudaFuncSetAttribute((const void*)cfgs[c].kern[st],
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)cfgs[c].smem));
     return AC_SUCCESS;
 }
 
@@ -212,21 +190,18 @@ prepare_kernels_once()
         return AC_SUCCESS;
     int n;
     const SolveConfig* cfgs = solve_configs(&n);
-    for (int c = 0; c < n; ++c)
-        for (int s = 0; s < 3; ++s)
-            ACB_CUDA_CHECK(cudaFuncSetAttribute((const void*)cfgs[c].kern[s],
-                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)cfgs[c].smem));
+    if (prepare_table(cfgs, n) != AC_SUCCESS)
+        return AC_FAILURE;
     done = true;
     return AC_SUCCESS;
 }
 
 // Kernel arguments from the uniform mirror (coefficients pre-scaled in double,
 // rounded once to AcReal).
-static SolveParams<AcReal>
-make_params(const Device d, int step)
+SolveParams<AcReal>
+acb_host::make_params(const AcMeshInfo& uniforms, const Layout& L, int step, int forcing)
 {
-    const AcReal* rp = d->uniforms.real_params;
+    const AcReal* rp = uniforms.real_params;
     SolveParams<AcReal> P;
     memset(&P, 0, sizeof(P));
     const double inv[3] = {rp[AC_inv_dsx], rp[AC_inv_dsy], rp[AC_inv_dsz]};
@@ -266,8 +241,8 @@ make_params(const Device d, int step)
     P.rkB                 = (AcReal)(beta[step] * dt);
     P.rkA                 = step > 0 ? (AcReal)(beta[step] * alpha[step] / beta[step - 1]) : 0;
 
-    P.forcing = d->forcing;
-    if (d->forcing) {
+    P.forcing = forcing;
+    if (forcing) {
         const double cs    = sqrt((double)rp[AC_cs2_sound]);
         const double kaver = rp[AC_kaver];
         const double NN    = cs * (double)rp[AC_forcing_magnitude] * sqrt(kaver * cs);
@@ -283,9 +258,9 @@ make_params(const Device d, int step)
         P.ff_im[2]         = rp[AC_ff_hel_imz];
         P.fcphi            = (AcReal)cos((double)rp[AC_forcing_phase]);
         P.fsphi            = (AcReal)sin((double)rp[AC_forcing_phase]);
-        const int3 gn      = d->uniforms.int3_params[AC_global_grid_n];
-        const int nn[3]    = {gn.x > 0 ? gn.x : d->L.nx, gn.y > 0 ? gn.y : d->L.ny,
-                           gn.z > 0 ? gn.z : d->L.nz};
+        const int3 gn      = uniforms.int3_params[AC_global_grid_n];
+        const int nn[3]    = {gn.x > 0 ? gn.x : L.nx, gn.y > 0 ? gn.y : L.ny,
+                           gn.z > 0 ? gn.z : L.nz};
         const double ds[3] = {rp[AC_dsx], rp[AC_dsy], rp[AC_dsz]};
         for (int c = 0; c < 3; ++c) {
             P.fds[c] = (AcReal)ds[c];
@@ -293,6 +268,28 @@ make_params(const Device d, int step)
         }
     }
     return P;
+}
+
+// Cuts z into 1..8 segments of at least `min_planes` planes so that the last
+// wave of (tile, segment) tasks is as full as possible; fewer segments win
+// near-ties because each segment re-reads 6 halo planes.
+int
+acb_host::choose_segments(long long ntiles, int nzr, long long slots, int min_planes)
+{
+    int best_seg    = 1;
+    double best_eff = -1.0;
+    for (int ns = 1; ns <= 8; ++ns) {
+        if (ns > 1 && nzr / ns < min_planes)
+            break;
+        const long long T    = ntiles * ns;
+        const long long wave = (T + slots - 1) / slots;
+        const double eff     = (double)T / (double)(wave * slots) - 0.01 * (ns - 1);
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best_seg = ns;
+        }
+    }
+    return best_seg;
 }
 
 static bool
@@ -331,24 +328,29 @@ launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e)
     g.ntx        = (e.x - 1 - NGHOST) / cfg.TX - g.tx0 + 1;
     g.nty        = (e.y - s.y + cfg.TY - 1) / cfg.TY;
     g.nzr        = e.z - s.z;
-    g.units      = (long long)g.ntx * g.nty * g.nzr;
     a.out        = d->blk[d->cur ^ 1];
     a.in_lo      = d->lo[d->cur];
     a.out_lo     = d->lo[d->cur ^ 1];
     a.status     = d->status;
-    a.P          = make_params(d, step);
+    a.P          = make_params(d->uniforms, d->L, step, d->forcing);
 
     int per_sm = 0;
     ACB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.kern[step],
                                                                  cfg.threads, cfg.smem));
     if (per_sm < 1)
         per_sm = 1;
-    long long grid = (long long)d->num_sms * per_sm;
-    if (grid > g.units)
-        grid = g.units;
+    const long long slots = (long long)d->num_sms * per_sm;
+    const long long ntiles = (long long)g.ntx * g.nty;
+    const int best_seg     = choose_segments(ntiles, g.nzr, slots, 16);
+    g.nseg  = best_seg;
+    g.zseg  = (g.nzr + best_seg - 1) / best_seg;
+    g.nseg  = (g.nzr + g.zseg - 1) / g.zseg;
+    g.tasks = ntiles * g.nseg;
+    long long grid = std::min(slots, g.tasks);
     cfg.kern[step]<<<(unsigned)grid, cfg.threads, cfg.smem, st>>>(d->tmap[d->cur], a);
     ACB_CUDA_CHECK(cudaGetLastError());
     d->launches++;
+    d->ghost_ok[d->cur ^ 1] = false; // the out block's ghosts are stale now
     return AC_SUCCESS;
 }
 
@@ -364,6 +366,21 @@ launch_halo(const Device d, cudaStream_t st, int3 s, int3 e, int f0, int f1)
     e.z             = std::min(e.z, L.mz);
     if (e.x <= s.x || e.y <= s.y || e.z <= s.z)
         return AC_SUCCESS;
+    if (d->ghost_ok[d->cur])
+        return AC_SUCCESS; // every ghost already holds its periodic image
+    const bool whole = f0 == 0 && f1 == NUM_VTXBUF_HANDLES && s.x == 0 && s.y == 0 && s.z == 0 &&
+                       e.x == L.mx && e.y == L.my && e.z == L.mz;
+    if (whole) {
+        const long long units = halo_units(L);
+        const long long want  = (units + 255) / 256;
+        const int blocks = (int)std::max(1LL, std::min(want, (long long)d->num_sms * 32));
+        halo_full_kernel<<<blocks, 256, 0, st>>>(L, d->blk[d->cur], d->lo[d->cur],
+                                                 (unsigned)halo_units_a(L), (unsigned)units);
+        ACB_CUDA_CHECK(cudaGetLastError());
+        d->launches++;
+        d->ghost_ok[d->cur] = true;
+        return AC_SUCCESS;
+    }
     HaloArgs a;
     a.L     = L;
     a.block = d->blk[d->cur];
@@ -448,11 +465,10 @@ for_each_row_run(const Layout& L, size_t s, size_t count, F fn)
     return AC_SUCCESS;
 }
 
-static AcResult
-copy_field_range(const Device d, cudaStream_t st, state_t* field, size_t s, AcReal* host,
-                 size_t count, bool h2d, float* lo_field)
+AcResult
+acb_host::copy_field_range(cudaStream_t st, const Layout& L, state_t* field, size_t s,
+                           AcReal* host, size_t count, bool h2d, float* lo_field)
 {
-    const Layout& L  = d->L;
     const size_t w   = sizeof(state_t);
     const size_t dpw = (size_t)L.mxp * w, hpw = (size_t)L.mx * w;
     return for_each_row_run(L, s, count, [&](size_t dev, size_t t, size_t n, size_t rows) {
@@ -843,6 +859,7 @@ acDeviceAutoOptimize(const Device device)
     device->solve_cfg = best;
     ACB_CUDA_CHECK(cudaMemcpyAsync(device->blk[device->cur ^ 1], save, bytes,
                                    cudaMemcpyDeviceToDevice, st));
+    device->ghost_ok[device->cur ^ 1] = false;
     ACB_CUDA_CHECK(cudaStreamSynchronize(st));
     cudaFree(save);
     cudaEventDestroy(t0);
@@ -871,7 +888,8 @@ acDeviceLoadVertexBufferWithOffset(const Device device, const Stream stream,
     const size_t didx = acVertexBufferIdx(dst.x, dst.y, dst.z, device->local_config);
     const Layout& L   = device->L;
     float* lo         = device->lo[device->cur] ? device->lo[device->cur] + h * L.fstride : nullptr;
-    return copy_field_range(device, stream_of(device, stream),
+    device->ghost_ok[device->cur] = false;
+    return copy_field_range(stream_of(device, stream), L,
                             device->blk[device->cur] + h * L.fstride, didx,
                             host_mesh.vertex_buffer[h] + sidx, (size_t)num_vertices, true, lo);
 }
@@ -915,6 +933,7 @@ acDeviceSetVertexBuffer(const Device device, const Stream stream, const VertexBu
     cudaSetDevice(device->id);
     const cudaStream_t st = stream_of(device, stream);
     // both in and out, as the reference does (src/core/device.cc:296-314)
+    device->ghost_ok[0] = device->ghost_ok[1] = false;
     for (int b = 0; b < 2; ++b)
         if (launch_pack(device, st, b, h, nullptr, 0, 1, (double)value) != AC_SUCCESS)
             return AC_FAILURE;
@@ -933,7 +952,7 @@ acDeviceStoreVertexBufferWithOffset(const Device device, const Stream stream,
     const size_t sidx = acVertexBufferIdx(src.x, src.y, src.z, device->local_config);
     const size_t didx = acVertexBufferIdx(dst.x, dst.y, dst.z, host_mesh->info);
     const Layout& L   = device->L;
-    return copy_field_range(device, stream_of(device, stream),
+    return copy_field_range(stream_of(device, stream), L,
                             device->blk[device->cur] + h * L.fstride, sidx,
                             host_mesh->vertex_buffer[h] + didx, (size_t)num_vertices, false,
                             nullptr);
@@ -1001,6 +1020,7 @@ acDeviceTransferVertexBufferWithOffset(const Device src_device, const Stream str
         return AC_FAILURE;
     }
     cudaSetDevice(src_device->id);
+    dst_device->ghost_ok[dst_device->cur] = false;
     transfer_kernel<<<src_device->num_sms * 4, 256, 0, stream_of(src_device, stream)>>>(
         src_device->L, src_device->blk[src_device->cur] + h * src_device->L.fstride,
         (long long)sidx, dst_device->L, dst_device->blk[dst_device->cur] + h * dst_device->L.fstride,
@@ -1294,11 +1314,13 @@ acDeviceIntegrateSteps(const Device device, const Stream stream, const AcReal dt
         return AC_FAILURE;
     const cudaStream_t st = stream_of(device, stream);
     // key: parameters, configuration and stream the graph was captured with
-    const unsigned long long key = (device->uniform_version << 8) ^
-                                   ((unsigned long long)device->solve_cfg << 1) ^
-                                   ((unsigned long long)stream << 40) ^ 1ull;
+    const unsigned long long base = (device->uniform_version << 8) ^
+                                    ((unsigned long long)device->solve_cfg << 2) ^
+                                    ((unsigned long long)stream << 40) ^ 1ull;
     for (int i = 0; i < num_steps; ++i) {
         const int p = device->cur;
+        // a captured step contains the ghost fill only when the ghosts were stale
+        const unsigned long long key = base ^ (device->ghost_ok[p] ? 2ull : 0ull);
         if (!device->graph[p] || device->graph_key[p] != key) {
             if (device->graph[p])
                 cudaGraphExecDestroy(device->graph[p]);
@@ -1308,8 +1330,11 @@ acDeviceIntegrateSteps(const Device device, const Stream stream, const AcReal dt
             const unsigned long long before = device->launches;
             const AcResult rc               = enqueue_step(device, st);
             ACB_CUDA_CHECK(cudaStreamEndCapture(st, &g));
-            device->cur      = p; // capture advanced the roles; replay does it below
-            device->launches = before;
+            device->cur               = p; // capture advanced the roles; replay does it below
+            device->graph_launches[p] = device->launches - before;
+            device->graph_ghost[p][0] = device->ghost_ok[0];
+            device->graph_ghost[p][1] = device->ghost_ok[1];
+            device->launches          = before;
             if (rc != AC_SUCCESS) {
                 cudaGraphDestroy(g);
                 return AC_FAILURE;
@@ -1319,7 +1344,9 @@ acDeviceIntegrateSteps(const Device device, const Stream stream, const AcReal dt
             device->graph_key[p] = key;
         }
         ACB_CUDA_CHECK(cudaGraphLaunch(device->graph[p], st));
-        device->launches += 6;
+        device->launches += device->graph_launches[p];
+        device->ghost_ok[0] = device->graph_ghost[p][0]; // as the captured step left them
+        device->ghost_ok[1] = device->graph_ghost[p][1];
         device->cur ^= 1; // three swaps per step
     }
     return AC_SUCCESS;
@@ -1336,6 +1363,7 @@ acDeviceLoadVertexBufferDouble(const Device device, const Stream stream,
         return AC_FAILURE;
     const cudaStream_t st = stream_of(device, stream);
     const size_t n        = (size_t)device->L.mx * device->L.my * device->L.mz;
+    device->ghost_ok[device->cur] = false;
     ACB_CUDA_CHECK(cudaMemcpyAsync(device->xfer, src, n * sizeof(double), cudaMemcpyHostToDevice, st));
     if (launch_pack(device, st, device->cur, h, device->xfer, 0, 0, 0.0) != AC_SUCCESS)
         return AC_FAILURE;

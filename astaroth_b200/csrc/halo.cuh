@@ -1,4 +1,4 @@
-// Periodic ghost-zone fill, all requested fields in one launch.
+// Periodic ghost-zone fill.
 //
 // Reference behaviour (src/core/kernels/boundconds.cuh:131-190): every ghost
 // vertex (i, j, k) of the box [start, end) takes the value of the interior
@@ -6,11 +6,22 @@
 // vertex, so all ghost vertices can be written concurrently.
 //
 // The reference launches one thread per vertex of the whole m^3 box per field
-// (8 launches per call) and returns early for the 96.5% interior threads. Here
-// one warp owns one (j, k) row of the box and loops over the fields:
-//   - a row whose j or k lies in the ghost zone is copied whole, lane-strided
-//     (coalesced) from its wrapped source row;
-//   - an interior row only has its 3 + 3 x-ghosts, filled by six lanes.
+// (8 launches per call) and returns early for the 96.5% interior threads.
+//
+// Whole-box fill (the case every integration step takes): the ghost vertices
+// split into two kinds of independent work units, all in one launch.
+//   A. interior rows (j, k both interior): only the 3 + 3 x-ghosts. One thread
+//      per (row, field) copies the six vertices of both halves (hi and lo in
+//      the mixed build): 6 or 12 independent loads before any store.
+//   B. ghost rows (j or k in the ghost zone): the whole row. One thread per
+//      (row, field, 128-vertex chunk, lane) copies four vertices 32 apart, so
+//      each warp instruction is one coalesced 128-byte row segment and each
+//      thread has 4 (8) loads in flight.
+// A thread never stores before all its loads are issued, so memory-level
+// parallelism comes from the thread count, not from the warp count per row.
+//
+// Sub-box fill (any start/end, any field range): one warp per (j, k) row of the
+// box, lane-strided; kept for the reference's partial-box API calls.
 #pragma once
 #include "common.cuh"
 
@@ -29,47 +40,218 @@ wrap_interior(int c, int n)
     return ((c - NGHOST + n) % n) + NGHOST;
 }
 
-__global__ void __launch_bounds__(256)
+// Fills the ghost vertices of row (j, k) of the box [start, end) for fields
+// [f0, f1), with the 32 lanes of one warp.
+__device__ __forceinline__ void
+halo_row(const Layout& L, state_t* block, float* lo, int3 start, int3 end, int f0, int f1, int j,
+         int k, int lane)
+{
+    const bool ghost_row = j < NGHOST || j >= NGHOST + L.ny || k < NGHOST || k >= NGHOST + L.nz;
+    const int js         = wrap_interior(j, L.ny);
+    const int ks         = wrap_interior(k, L.nz);
+    const long long drow = lidx(L, 0, j, k);
+    const long long srow = lidx(L, 0, js, ks);
+    if (ghost_row) {
+        for (int f = f0; f < f1; ++f) {
+            state_t* F = block + f * L.fstride;
+            for (int i = start.x + lane; i < end.x; i += 32)
+                F[drow + i] = F[srow + wrap_interior(i, L.nx)];
+            if (ACB_MIXED && lo) {
+                float* G = lo + f * L.fstride;
+                for (int i = start.x + lane; i < end.x; i += 32)
+                    G[drow + i] = G[srow + wrap_interior(i, L.nx)];
+            }
+        }
+    }
+    else if (lane < 2 * NGHOST) {
+        const int i = lane < NGHOST ? lane : L.nx + lane; // 0,1,2 and nx+3..nx+5
+        if (i >= start.x && i < end.x) {
+            const int is = wrap_interior(i, L.nx);
+            for (int f = f0; f < f1; ++f) {
+                state_t* F = block + f * L.fstride;
+                F[drow + i] = F[srow + is];
+                if (ACB_MIXED && lo) {
+                    float* G = lo + f * L.fstride;
+                    G[drow + i] = G[srow + is];
+                }
+            }
+        }
+    }
+}
+
+static __global__ void __launch_bounds__(256)
 halo_kernel(const HaloArgs a)
 {
-    const Layout& L  = a.L;
-    const int lane   = threadIdx.x & 31;
+    const int lane       = threadIdx.x & 31;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const int ry = a.end.y - a.start.y;
     for (long long r = warp; r < a.rows; r += nwarps) {
         const int j = a.start.y + (int)(r % ry);
         const int k = a.start.z + (int)(r / ry);
-        const bool ghost_row = j < NGHOST || j >= NGHOST + L.ny || k < NGHOST || k >= NGHOST + L.nz;
-        const int js = wrap_interior(j, L.ny);
-        const int ks = wrap_interior(k, L.nz);
-        const long long drow = lidx(L, 0, j, k);
-        const long long srow = lidx(L, 0, js, ks);
-        if (ghost_row) {
-            for (int f = a.f0; f < a.f1; ++f) {
-                state_t* F = a.block + f * L.fstride;
-                for (int i = a.start.x + lane; i < a.end.x; i += 32)
-                    F[drow + i] = F[srow + wrap_interior(i, L.nx)];
-                if (ACB_MIXED && a.lo) {
-                    float* G = a.lo + f * L.fstride;
-                    for (int i = a.start.x + lane; i < a.end.x; i += 32)
-                        G[drow + i] = G[srow + wrap_interior(i, L.nx)];
-                }
-            }
+        halo_row(a.L, a.block, a.lo, a.start, a.end, a.f0, a.f1, j, k, lane);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Whole-box fill of all fields (n >= NGHOST on every axis).
+
+// 128-vertex chunks per ghost row.
+__host__ __device__ __forceinline__ unsigned
+halo_chunks(const Layout& L)
+{
+    return (unsigned)(L.mx + 127) / 128;
+}
+
+// Work units of kind A (interior rows x fields) and A + B of one mesh.
+static inline long long
+halo_units_a(const Layout& L)
+{
+    return (long long)L.ny * L.nz * ACB_NF;
+}
+
+static inline long long
+halo_units(const Layout& L)
+{
+    const long long ghost_rows = (long long)L.my * L.mz - (long long)L.ny * L.nz;
+    return halo_units_a(L) + ghost_rows * ACB_NF * halo_chunks(L) * 32;
+}
+
+// Periodic source of ghost-or-interior coordinate c in [0, n + 6), n >= NGHOST.
+__device__ __forceinline__ int
+wrap_near(int c, int n)
+{
+    return c < NGHOST ? c + n : (c >= n + NGHOST ? c - n : c);
+}
+
+__device__ __forceinline__ void
+halo_unit(const Layout& L, state_t* block, float* lo, unsigned units_a, unsigned u)
+{
+    if (u < units_a) {
+        // kind A: x-ghosts of interior row r, field f
+        const unsigned f     = u % ACB_NF;
+        const unsigned r     = u / ACB_NF;
+        const unsigned kq    = r / (unsigned)L.ny;
+        const int j          = NGHOST + (int)(r - kq * (unsigned)L.ny);
+        const int k          = NGHOST + (int)kq;
+        const long long base = lidx(L, 0, j, k) + (long long)f * L.fstride;
+        state_t* F           = block + base;
+        state_t v[2 * NGHOST];
+#pragma unroll
+        for (int q = 0; q < NGHOST; ++q) {
+            v[q]          = F[L.nx + q]; // source of ghost q is nx + q
+            v[NGHOST + q] = F[NGHOST + q]; // source of ghost nx + 3 + q is 3 + q
         }
-        else if (lane < 2 * NGHOST) {
-            const int i = lane < NGHOST ? lane : L.nx + lane; // 0,1,2 and nx+3..nx+5
-            if (i >= a.start.x && i < a.end.x) {
-                const int is = wrap_interior(i, L.nx);
-                for (int f = a.f0; f < a.f1; ++f) {
-                    state_t* F = a.block + f * L.fstride;
-                    F[drow + i] = F[srow + is];
-                    if (ACB_MIXED && a.lo) {
-                        float* G = a.lo + f * L.fstride;
-                        G[drow + i] = G[srow + is];
-                    }
-                }
-            }
+#if ACB_MIXED
+        float* G = lo + base;
+        float w[2 * NGHOST];
+#pragma unroll
+        for (int q = 0; q < NGHOST; ++q) {
+            w[q]          = G[L.nx + q];
+            w[NGHOST + q] = G[NGHOST + q];
         }
+#endif
+#pragma unroll
+        for (int q = 0; q < NGHOST; ++q) {
+            F[q]                   = v[q];
+            F[L.nx + NGHOST + q]   = v[NGHOST + q];
+#if ACB_MIXED
+            G[q]                   = w[q];
+            G[L.nx + NGHOST + q]   = w[NGHOST + q];
+#endif
+        }
+        return;
+    }
+    // kind B: 4 vertices, 32 apart, of a 128-vertex chunk of ghost row `row`
+    u -= units_a;
+    const unsigned lane = u & 31;
+    unsigned wq         = u >> 5;
+    const unsigned f    = wq % ACB_NF;
+    wq /= ACB_NF;
+    const unsigned nch   = halo_chunks(L);
+    const unsigned row   = wq / nch;
+    const unsigned chunk = wq - row * nch;
+    // ghost rows: first the 6 ghost z planes (all j), then the 6 ghost j rows
+    // of every interior z plane
+    const unsigned zrows = 2 * NGHOST * (unsigned)L.my;
+    int j, k;
+    if (row < zrows) {
+        const unsigned kk = row / (unsigned)L.my;
+        j                 = (int)(row - kk * (unsigned)L.my);
+        k                 = kk < NGHOST ? (int)kk : L.nz + (int)kk;
+    }
+    else {
+        const unsigned r  = row - zrows;
+        const unsigned kk = r / (2 * NGHOST);
+        const unsigned jj = r - kk * (2 * NGHOST);
+        k                 = NGHOST + (int)kk;
+        j                 = jj < NGHOST ? (int)jj : L.ny + (int)jj;
+    }
+    const long long fo = (long long)f * L.fstride;
+    const long long d  = fo + lidx(L, 0, j, k);
+    const long long s  = fo + lidx(L, 0, wrap_near(j, L.ny), wrap_near(k, L.nz));
+    const int x0       = (int)(chunk * 128 + lane);
+    state_t v[4];
+#if ACB_MIXED
+    float w[4];
+#endif
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int x = x0 + 32 * q;
+        if (x < L.mx) {
+            const int xs = wrap_near(x, L.nx);
+            v[q]         = block[s + xs];
+#if ACB_MIXED
+            w[q] = lo[s + xs];
+#endif
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int x = x0 + 32 * q;
+        if (x < L.mx) {
+            block[d + x] = v[q];
+#if ACB_MIXED
+            lo[d + x] = w[q];
+#endif
+        }
+    }
+}
+
+static __global__ void __launch_bounds__(256)
+halo_full_kernel(const Layout L, state_t* block, float* lo, unsigned units_a, unsigned units)
+{
+    const unsigned stride = gridDim.x * blockDim.x;
+    for (unsigned u = blockIdx.x * blockDim.x + threadIdx.x; u < units; u += stride)
+        halo_unit(L, block, lo, units_a, u);
+}
+
+// One member of a batched ghost fill (whole m-box of every field).
+struct HaloMember {
+    Layout L;
+    state_t* block;
+    float* lo;
+    long long unit_begin; // first global work unit of this member
+    unsigned units_a;     // its kind-A units
+};
+
+// Ghost fill of every field of many meshes in one launch; threads take the
+// concatenated work units of all members.
+static __global__ void __launch_bounds__(256)
+halo_batch_kernel(const HaloMember* __restrict__ mem, int n, long long total_units)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < total_units;
+         u += stride) {
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (mem[mid].unit_begin <= u)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const HaloMember& m = mem[lo];
+        halo_unit(m.L, m.block, m.lo, m.units_a, (unsigned)(u - m.unit_begin));
     }
 }

@@ -1,0 +1,75 @@
+// Host-side pieces shared by the Device layer (device.cu) and the ensemble
+// (ensemble.cu): the table of compiled solve-kernel tile shapes, tensor-map
+// encoding, kernel arguments from a parameter mirror, the work split, and the
+// flat <-> padded copies.
+#pragma once
+#include "astaroth.h"
+#include "common.cuh"
+#include "solve.cuh"
+
+// Solve tile shapes (tile width, tile height, ring depth, CTAs per SM hint)
+#if AC_DOUBLE_PRECISION == 1
+using SolveCfg0 = TileCfg<32, 4, 8, 1>;
+using SolveCfg1 = TileCfg<16, 8, 8, 1>;
+using SolveCfg2 = TileCfg<32, 2, 10, 2>;
+#else
+using SolveCfg0 = TileCfg<32, 8, 9, 1>;
+using SolveCfg1 = TileCfg<32, 4, 10, 1>;
+using SolveCfg2 = TileCfg<64, 4, 8, 1>;
+#endif
+
+typedef void (*SolveKernelFn)(const CUtensorMap, const SolveArgs<AcReal>);
+
+struct SolveConfig {
+    const char* name;
+    int TX, TY, NP, threads;
+    size_t smem;
+    SolveKernelFn kern[3]; // substeps 0, 1, 2
+};
+
+template <class Cfg, bool ENS>
+SolveConfig
+make_solve_config(const char* name)
+{
+    SolveConfig c;
+    c.name    = name;
+    c.TX      = Cfg::TX;
+    c.TY      = Cfg::TY;
+    c.NP      = Cfg::NP;
+    c.threads = Cfg::THREADS;
+    c.smem    = Cfg::smem_bytes();
+    c.kern[0] = solve_kernel<Cfg, 0, ENS>;
+    c.kern[1] = solve_kernel<Cfg, 1, ENS>;
+    c.kern[2] = solve_kernel<Cfg, 2, ENS>;
+    return c;
+}
+
+namespace acb_host {
+
+constexpr int kDefaultSolveConfig = 0;
+
+// single-mesh kernels (device.cu) and ensemble kernels (ensemble.cu), same tiles
+const SolveConfig* solve_configs(int* n);
+const SolveConfig* ensemble_configs(int* n);
+
+// raises the dynamic shared-memory limit of every kernel of a table, once
+AcResult prepare_table(const SolveConfig* cfgs, int n);
+
+// 4-D map (x, y, z, field) over a field block with a (TX+8, TY+6, 1, 8) box
+AcResult encode_block_map(const Layout& L, const state_t* block, const SolveConfig& cfg,
+                          CUtensorMap* map);
+
+// kernel arguments from a parameter mirror: coefficients pre-scaled in double
+// and rounded once to AcReal; rkA/rkB for `step` from AC_dt
+SolveParams<AcReal> make_params(const AcMeshInfo& uniforms, const Layout& L, int step,
+                                int forcing);
+
+// z segments per tile column so that tiles*segments fills the last wave best
+int choose_segments(long long ntiles, int nzr, long long slots, int min_planes);
+
+// copies a flat range of a field between host memory (reference order) and
+// the padded device layout; zeroes the lo parts of loaded values when given
+AcResult copy_field_range(cudaStream_t st, const Layout& L, state_t* field, size_t s,
+                          AcReal* host, size_t count, bool h2d, float* lo_field);
+
+} // namespace acb_host

@@ -13,14 +13,17 @@
 //
 // B200 structure (no counterpart in the reference, which reads 55 stencil points
 // per field straight from global memory with one thread per vertex):
-//   - persistent CTAs: the (x-y tile, z-plane) work of the region is linearised
-//     and split into equal contiguous ranges, one per CTA, so the grid is a
-//     multiple of the SM count and the tail is at most one plane per CTA;
-//   - each CTA streams its tile along z (2.5D): one TMA load per plane brings
-//     all eight fields of a (TX+8) x (TY+6) halo'd tile into a ring of NP
-//     plane slots in shared memory, NP - 7 planes ahead of the consumer;
-//   - one thread per (x, y) column; every stencil operand, including the
-//     z-neighbours and the xz/yz diagonals, is read from the ring;
+//   - persistent CTAs (one per SM slot) take tasks = (x-y tile, z segment)
+//     round-robin, segment-major, so the CTAs of one wave stream neighbouring
+//     tiles at the same z and read each other's halo planes from L2;
+//   - each CTA streams its tile along z (2.5D): a producer warp issues one TMA
+//     load per plane bringing all eight fields of a (TX+8) x (TY+6) halo'd tile
+//     into a ring of NP plane slots in shared memory (mbarrier `full` with
+//     transaction bytes); consumer warps release a slot through an `empty`
+//     mbarrier when done, so no block-wide barrier sits in the plane loop;
+//   - one consumer thread per (x, y) column; every stencil operand, including
+//     the z-neighbours and the xz/yz diagonals, is read from the ring; the
+//     centre-only values (previous state, lo parts) are loaded a plane ahead;
 //   - derivative coefficients arrive pre-scaled by 1/ds (and 1/ds^2) so each
 //     pencil costs 6-7 FP ops; only the 21 first, 24 second and 12 cross
 //     derivatives the right-hand sides use are formed;
@@ -50,7 +53,23 @@ struct SolveGeom {
                      // so that every TMA box starts on a 16-byte boundary
     int ntx, nty;    // tiles covering the region
     int nzr;         // planes of the region
-    long long units; // ntx * nty * nzr
+    int zseg;        // planes per task (the region's z range is cut into nseg segments)
+    int nseg;
+    long long tasks; // ntx * nty * nseg; task t = (segment t / tiles, tile t % tiles)
+};
+
+// One member of an ensemble (many independent meshes advanced by one launch):
+// the TMA map of its `in` block, its geometry and task range, its buffers and
+// its parameters. Kept in global memory, one table per buffer parity.
+template <typename T>
+struct __align__(128) MemberDesc {
+    CUtensorMap tmap;
+    SolveGeom g;
+    long long task_begin; // first global task of this member (tasks are member-major)
+    state_t* out;
+    float* in_lo;
+    float* out_lo;
+    SolveParams<T> P; // rkA / rkB / forcing are taken from the launch, not from here
 };
 
 template <typename T>
@@ -61,13 +80,19 @@ struct SolveArgs {
     float* out_lo;   // mixed build: lo parts of `out`
     unsigned* status;
     SolveParams<T> P;
+    // ensemble launches only
+    const MemberDesc<T>* members;
+    int nmembers;
+    long long total_tasks;
 };
 
 template <int TX_, int TY_, int NP_, int MINB_>
 struct TileCfg {
     static constexpr int TX = TX_, TY = TY_, NP = NP_, MINB = MINB_;
     static constexpr int BX = TX_ + 8, BY = TY_ + 6;
-    static constexpr int THREADS = TX_ * TY_;
+    static constexpr int CONSUMERS = TX_ * TY_;        // one thread per (x, y) column
+    static constexpr int CWARPS    = CONSUMERS / 32;   // consumer warps
+    static constexpr int THREADS   = CONSUMERS + 32;   // plus one producer warp
     static constexpr int FIELD   = BX * BY;
     static constexpr int PLANE   = ACB_NF * FIELD; // elements per ring slot
     static constexpr size_t smem_bytes() { return (size_t)NP * PLANE * sizeof(state_t); }
@@ -332,160 +357,298 @@ pair_add(float hi, float lo, float d, float& ohi, float& olo)
 
 } // namespace acb
 
-template <class Cfg, int STEP>
+// Values of the vertex's own column that the update needs besides the ring:
+// the previous state (s > 0) and, in the mixed build, the lo parts.
+struct CentreVals {
+    AcReal prev[ACB_NF];
+    float cur_lo[ACB_NF];
+    float prev_lo[ACB_NF];
+};
+
+template <int STEP>
+__device__ __forceinline__ void
+load_centre(const Layout& L, const state_t* out, const float* in_lo, const float* out_lo,
+            long long id, CentreVals& c)
+{
+    const long long fs = L.fstride;
+#pragma unroll
+    for (int f = 0; f < ACB_NF; ++f) {
+        if (STEP > 0)
+            c.prev[f] = out[f * fs + id];
+#if ACB_MIXED
+        c.cur_lo[f]  = in_lo[f * fs + id];
+        c.prev_lo[f] = STEP > 0 ? out_lo[f * fs + id] : 0.f;
+#endif
+    }
+}
+
+template <class Cfg>
+struct TaskGeom {
+    int i0, j0, k0, nout;
+    __device__ __forceinline__ TaskGeom(const SolveGeom& g, long long t, long long ntiles)
+    {
+        const long long seg  = t / ntiles;
+        const long long tile = t - seg * ntiles;
+        const int tile_x     = (int)(tile % g.ntx);
+        const int tile_y     = (int)(tile / g.ntx);
+        i0                   = NGHOST + (g.tx0 + tile_x) * Cfg::TX;
+        j0                   = g.start.y + tile_y * Cfg::TY;
+        k0                   = g.start.z + (int)seg * g.zseg;
+        nout                 = min(g.zseg, g.nzr - (int)seg * g.zseg);
+    }
+};
+
+__device__ __forceinline__ void
+fence_tensormap_acquire(const CUtensorMap* map)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(
+                     reinterpret_cast<uint64_t>(map))
+                 : "memory");
+}
+
+// Which member an ensemble task belongs to (binary search on task_begin).
+template <typename T>
+__device__ __forceinline__ int
+member_of(const MemberDesc<T>* md, int n, long long t)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (md[mid].task_begin <= t)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+
+// One task of a consumer warp: the planes of one (tile, z segment) column.
+// Waits for the ring, computes and stores every output plane, releases the
+// slots, and advances the plane counter q. Returns false if the CTA aborts.
+template <class Cfg, int STEP, bool ENS>
+__device__ __forceinline__ bool
+consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<AcReal>& P,
+             long long lt, state_t* out, float* in_lo, float* out_lo, const state_t* ring,
+             uint64_t* full, uint64_t* empty, volatile int* abort_flag, uint32_t& q)
+{
+    using T = AcReal;
+    constexpr int TX = Cfg::TX, NP = Cfg::NP, BX = Cfg::BX;
+    constexpr int FIELD = Cfg::FIELD, PLANE = Cfg::PLANE;
+    const int tid  = threadIdx.x;
+    const int lane = tid & 31;
+    const int tx   = tid % TX;
+    const int ty   = tid / TX;
+    const Layout& L = gv.L;
+    const TaskGeom<Cfg> tg(gv, lt, (long long)gv.ntx * gv.nty);
+    const int nload = tg.nout + 2 * NGHOST;
+    const int i     = tg.i0 + tx;
+    const int j     = tg.j0 + ty;
+    const bool act  = (i >= gv.start.x) && (i < gv.end.x) && (j < gv.end.y);
+    const T rkA     = a.P.rkA, rkB = a.P.rkB;
+
+    bool ok = true;
+    for (int l = 0; l < 2 * NGHOST && ok; ++l)
+        ok = mbar_wait_bounded(&full[(q + l) % NP], ((q + l) / NP) & 1u);
+    ok = __all_sync(0xffffffffu, ok);
+
+    CentreVals cv;
+    if (act)
+        load_centre<STEP>(L, out, in_lo, out_lo, lidx(L, i, j, tg.k0), cv);
+
+    for (int p = 0; p < tg.nout; ++p) {
+        if (ok) {
+            const uint32_t l = q + p + 2 * NGHOST;
+            ok = mbar_wait_bounded(&full[l % NP], (l / NP) & 1u);
+            ok = __all_sync(0xffffffffu, ok);
+        }
+        if (!ok || *abort_flag) {
+            if (lane == 0) {
+                atomicOr(a.status, (unsigned)ACB_STATUS_TMA_TIMEOUT);
+                *abort_flag = 1;
+            }
+            return false;
+        }
+        const int k = tg.k0 + p;
+        CentreVals nx_cv; // next plane's centre values, loaded a plane ahead
+        if (act && p + 1 < tg.nout)
+            load_centre<STEP>(L, out, in_lo, out_lo, lidx(L, i, j, k + 1), nx_cv);
+        if (act) {
+            const uint32_t sc = (q + p + NGHOST) % NP;
+            int zo[7];
+#pragma unroll
+            for (int dz = -NGHOST; dz <= NGHOST; ++dz) {
+                const int sd    = (int)((q + p + NGHOST + dz) % NP);
+                zo[dz + NGHOST] = (sd - (int)sc) * PLANE;
+            }
+            const state_t* c = ring + (size_t)sc * PLANE + (ty + NGHOST) * BX + (tx + 4);
+            const long long id = lidx(L, i, j, k);
+
+            T roc[ACB_NF], cur[ACB_NF];
+            acb::mhd_rhs<T, BX, FIELD>(c, zo, P, roc, cur);
+
+            T fo[3] = {0, 0, 0};
+            if (!ENS && STEP == 2 && a.P.forcing)
+                acb::forcing_at<T>(a.P, i, j, k, fo);
+
+#pragma unroll
+            for (int f = 0; f < ACB_NF; ++f) {
+#if ACB_MIXED
+                float d = rkB * roc[f];
+                if (STEP > 0)
+                    d += rkA * ((cur[f] - cv.prev[f]) + (cv.cur_lo[f] - cv.prev_lo[f]));
+                float hi, lo;
+                acb::pair_add(cur[f], cv.cur_lo[f], d, hi, lo);
+                if (STEP == 2 && f >= 1 && f <= 3)
+                    acb::pair_add(hi, lo, fo[f - 1], hi, lo);
+                out[f * L.fstride + id]    = hi;
+                out_lo[f * L.fstride + id] = lo;
+#else
+                T r;
+                if (STEP == 0)
+                    r = cur[f] + rkB * roc[f];
+                else
+                    r = cur[f] + rkA * (cur[f] - cv.prev[f]) + rkB * roc[f];
+                if (STEP == 2 && f >= 1 && f <= 3)
+                    r += fo[f - 1];
+                out[f * L.fstride + id] = r;
+#endif
+            }
+        }
+        cv = nx_cv;
+        __syncwarp();
+        if (lane == 0)
+            mbar_arrive(&empty[(q + p) % NP]); // this warp is done with plane p
+    }
+    // the task's last six planes are no longer needed either
+    __syncwarp();
+    if (lane == 0)
+        for (int l = tg.nout; l < nload; ++l)
+            mbar_arrive(&empty[(q + l) % NP]);
+    q += nload;
+    return true;
+}
+
+// Warp-specialised pipeline. Warp CWARPS is the producer: one lane issues one
+// TMA load per plane (all 8 fields of the halo'd tile) into a ring of NP
+// slots, each guarded by a `full` barrier (transaction bytes) and an `empty`
+// barrier on which every consumer warp arrives once it has finished with the
+// plane. Consumer warps own one vertex column each and never wait for each
+// other except through the ring. Tasks (tile, z segment) are dealt round-robin
+// so the CTAs of one wave stream neighbouring tiles at the same z and their
+// halo reads of each other's planes hit L2. With ENS the tasks of all members
+// of an ensemble form one list (member-major) and each task reads its member's
+// map, geometry, buffers and parameters from the descriptor table.
+template <class Cfg, int STEP, bool ENS>
 __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     solve_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ SolveArgs<AcReal> a)
 {
     using T = AcReal;
-    constexpr int TX = Cfg::TX, TY = Cfg::TY, NP = Cfg::NP, BX = Cfg::BX;
-    constexpr int FIELD = Cfg::FIELD, PLANE = Cfg::PLANE;
+    constexpr int TX = Cfg::TX, NP = Cfg::NP, BX = Cfg::BX;
+    constexpr int FIELD = Cfg::FIELD, PLANE = Cfg::PLANE, CWARPS = Cfg::CWARPS;
     constexpr uint32_t PLANE_BYTES = PLANE * sizeof(state_t);
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     state_t* ring = reinterpret_cast<state_t*>(smem_raw);
-    __shared__ __align__(8) uint64_t bars[NP];
-    __shared__ int abort_flag;
+    __shared__ __align__(8) uint64_t full[NP];
+    __shared__ __align__(8) uint64_t empty[NP];
+    __shared__ volatile int abort_flag;
+    __shared__ SolveParams<T> sP[CWARPS]; // ensemble: each consumer warp's copy of its member's parameters
 
-    const int tid = threadIdx.x;
-    const int tx  = tid % TX;
-    const int ty  = tid / TX;
+    const int tid  = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
     if (tid == 0) {
-        for (int s = 0; s < NP; ++s)
-            mbar_init(&bars[s], 1);
+        for (int s = 0; s < NP; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], CWARPS);
+        }
         fence_barrier_init();
         abort_flag = 0;
-        prefetch_tensormap(&tin);
     }
     __syncthreads();
 
-    const SolveGeom& g = a.g;
-    const Layout& L    = g.L;
-    const long long U  = g.units;
-    const long long u0 = U * blockIdx.x / gridDim.x;
-    const long long u1 = U * (blockIdx.x + 1) / gridDim.x;
+    const long long ntasks = ENS ? a.total_tasks : a.g.tasks;
 
-    uint32_t q = 0; // planes this CTA has consumed the ring for so far
-    long long u = u0;
-    while (u < u1) {
-        const long long tile = u / g.nzr;
-        const int za         = (int)(u - tile * g.nzr);
-        const int zb         = (int)min((long long)g.nzr, za + (u1 - u));
-        u += zb - za;
-        const int tile_x = (int)(tile % g.ntx);
-        const int tile_y = (int)(tile / g.ntx);
-        const int i0     = NGHOST + (g.tx0 + tile_x) * TX;
-        const int j0     = g.start.y + tile_y * TY;
-        const int k0     = g.start.z + za;
-        const int nout   = zb - za;
-        const int nload  = nout + 2 * NGHOST;
-        const int xt     = L.offx + i0 - 4; // multiple of 16 bytes by construction
-        const int yt     = j0 - NGHOST;
-
-        int issued = 0;
-        if (tid == 0) {
-            const int first = nload < NP ? nload : NP;
-            for (int l = 0; l < first; ++l) {
-                const uint32_t s = (q + l) % NP;
-                mbar_arrive_expect_tx(&bars[s], PLANE_BYTES);
-                tma_load_4d(ring + (size_t)s * PLANE, &tin, xt, yt, k0 - NGHOST + l, 0, &bars[s]);
-            }
-            issued = first;
-        }
-        // the first output needs planes 0..6
-        bool ok = true;
-        for (int l = 0; l < 2 * NGHOST && ok; ++l)
-            ok = mbar_wait_bounded(&bars[(q + l) % NP], ((q + l) / NP) & 1u);
-
-        const int i    = i0 + tx;
-        const int j    = j0 + ty;
-        const bool act = (i >= g.start.x) && (i < g.end.x) && (j < g.end.y);
-
-        for (int p = 0; p < nout; ++p) {
-            if (ok) {
-                const uint32_t l = p + 2 * NGHOST;
-                ok               = mbar_wait_bounded(&bars[(q + l) % NP], ((q + l) / NP) & 1u);
+    if (warp == CWARPS) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            if (!ENS)
+                prefetch_tensormap(&tin);
+            uint32_t q  = 0;
+            bool ok     = true;
+            int last_m  = -1;
+            for (long long t = blockIdx.x; t < ntasks && ok; t += gridDim.x) {
+                const CUtensorMap* map = &tin;
+                const SolveGeom* g     = &a.g;
+                long long lt           = t;
+                if (ENS) {
+                    const int m                = member_of(a.members, a.nmembers, t);
+                    const MemberDesc<T>* md    = a.members + m;
+                    map                        = &md->tmap;
+                    g                          = &md->g;
+                    lt                         = t - md->task_begin;
+                    if (m != last_m) {
+                        fence_tensormap_acquire(map);
+                        prefetch_tensormap(map);
+                        last_m = m;
+                    }
+                }
+                const TaskGeom<Cfg> tg(*g, lt, (long long)g->ntx * g->nty);
+                const int xt    = g->L.offx + tg.i0 - 4; // a multiple of 16 bytes by construction
+                const int yt    = tg.j0 - NGHOST;
+                const int nload = tg.nout + 2 * NGHOST;
+                for (int l = 0; l < nload; ++l) {
+                    const uint32_t s = q % NP, use = q / NP;
+                    if (use > 0 && !mbar_wait_bounded(&empty[s], (use - 1) & 1u)) {
+                        ok = false;
+                        break;
+                    }
+                    if (abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&full[s], PLANE_BYTES);
+                    tma_load_4d(ring + (size_t)s * PLANE, map, xt, yt, tg.k0 - NGHOST + l, 0,
+                                &full[s]);
+                    ++q;
+                }
             }
             if (!ok) {
                 atomicOr(a.status, (unsigned)ACB_STATUS_TMA_TIMEOUT);
                 abort_flag = 1;
-            }
-            if (ok && act) {
-                const int k      = k0 + p;
-                const uint32_t sc = (q + p + NGHOST) % NP;
-                int zo[7];
-#pragma unroll
-                for (int dz = -NGHOST; dz <= NGHOST; ++dz) {
-                    const int sd   = (int)((q + p + NGHOST + dz) % NP);
-                    zo[dz + NGHOST] = (sd - (int)sc) * PLANE;
-                }
-                const state_t* c = ring + (size_t)sc * PLANE + (ty + NGHOST) * BX + (tx + 4);
-                const long long id = lidx(L, i, j, k);
-
-                T prev[ACB_NF];
-                if (STEP > 0) {
-#pragma unroll
-                    for (int f = 0; f < ACB_NF; ++f)
-                        prev[f] = a.out[f * L.fstride + id];
-                }
-#if ACB_MIXED
-                float cur_lo[ACB_NF], prev_lo[ACB_NF];
-#pragma unroll
-                for (int f = 0; f < ACB_NF; ++f) {
-                    cur_lo[f]  = a.in_lo[f * L.fstride + id];
-                    prev_lo[f] = STEP > 0 ? a.out_lo[f * L.fstride + id] : 0.f;
-                }
-#endif
-                T roc[ACB_NF], cur[ACB_NF];
-                acb::mhd_rhs<T, BX, FIELD>(c, zo, a.P, roc, cur);
-
-                T fo[3] = {0, 0, 0};
-                if (STEP == 2 && a.P.forcing)
-                    acb::forcing_at<T>(a.P, i, j, k, fo);
-
-#pragma unroll
-                for (int f = 0; f < ACB_NF; ++f) {
-#if ACB_MIXED
-                    float d = a.P.rkB * roc[f];
-                    if (STEP > 0)
-                        d += a.P.rkA * ((cur[f] - prev[f]) + (cur_lo[f] - prev_lo[f]));
-                    float hi, lo;
-                    acb::pair_add(cur[f], cur_lo[f], d, hi, lo);
-                    if (STEP == 2 && f >= 1 && f <= 3)
-                        acb::pair_add(hi, lo, fo[f - 1], hi, lo);
-                    a.out[f * L.fstride + id]    = hi;
-                    a.out_lo[f * L.fstride + id] = lo;
-#else
-                    T r;
-                    if (STEP == 0)
-                        r = cur[f] + a.P.rkB * roc[f];
-                    else
-                        r = cur[f] + a.P.rkA * (cur[f] - prev[f]) + a.P.rkB * roc[f];
-                    if (STEP == 2 && f >= 1 && f <= 3)
-                        r += fo[f - 1];
-                    a.out[f * L.fstride + id] = r;
-#endif
-                }
-            }
-            __syncthreads(); // every thread is done with plane p: its slot may be refilled
-            if (abort_flag)
-                break;
-            if (tid == 0 && issued < nload) {
-                const uint32_t l = issued; // == p + NP
-                const uint32_t s = (q + l) % NP;
-                fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&bars[s], PLANE_BYTES);
-                tma_load_4d(ring + (size_t)s * PLANE, &tin, xt, yt, k0 - NGHOST + l, 0, &bars[s]);
-                ++issued;
+                // wait (bounded) for this CTA's loads still in flight before leaving
+                for (uint32_t r = q > (uint32_t)NP ? q - NP : 0; r < q; ++r)
+                    (void)mbar_wait_bounded(&full[r % NP], (r / NP) & 1u);
             }
         }
-        if (abort_flag) {
-            // drain (bounded) whatever this CTA still has in flight, then leave
-            if (tid == 0) {
-                for (int l = issued > NP ? issued - NP : 0; l < issued; ++l)
-                    (void)mbar_wait_bounded(&bars[(q + l) % NP], ((q + l) / NP) & 1u);
-            }
+        return;
+    }
+
+    // ---------------------------------------------------------------- consumers
+    uint32_t q = 0;
+    for (long long t = blockIdx.x; t < ntasks; t += gridDim.x) {
+        bool ok;
+        if constexpr (ENS) {
+            const int m             = member_of(a.members, a.nmembers, t);
+            const MemberDesc<T>* md = a.members + m;
+            // each warp keeps its own copy, so no barrier across warps is needed
+            __syncwarp();
+            const int* srcw = reinterpret_cast<const int*>(&md->P);
+            int* dstw       = reinterpret_cast<int*>(&sP[warp]);
+            for (int w = lane; w < (int)(sizeof(SolveParams<T>) / sizeof(int)); w += 32)
+                dstw[w] = srcw[w];
+            __syncwarp();
+            const SolveGeom gv = md->g;
+            ok = consume_task<Cfg, STEP, ENS>(a, gv, sP[warp], t - md->task_begin, md->out,
+                                              md->in_lo, md->out_lo, ring, full, empty,
+                                              &abort_flag, q);
+        }
+        else {
+            ok = consume_task<Cfg, STEP, ENS>(a, a.g, a.P, t, a.out, a.in_lo, a.out_lo, ring, full,
+                                              empty, &abort_flag, q);
+        }
+        if (!ok)
             return;
-        }
-        q += nload;
     }
 }

@@ -45,6 +45,13 @@ mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
                  : "memory");
 }
 
+// Plain arrival (no transaction bytes), e.g. a consumer warp releasing a slot.
+__device__ __forceinline__ void
+mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ uint32_t
 mbar_try_wait(uint64_t* bar, uint32_t parity)
 {

@@ -189,3 +189,76 @@ class Device:
         _check(self.lib.acDeviceGetMemoryFootprint(self.handle, C.byref(b)),
                "acDeviceGetMemoryFootprint")
         return b.value
+
+
+class Ensemble:
+    """Python mirror of the ensemble entry points (include/astaroth_b200.h):
+    many independent meshes advanced by one launch per substep."""
+
+    def __init__(self, flavour: str, infos, device_id: int = 0):
+        self.flavour = flavour
+        self.prec = abi.PRECISIONS[flavour]
+        self.lib = library.load(flavour)
+        Info = abi.info_type(self.prec)
+        arr = (Info * len(infos))(*infos)
+        self.infos = list(infos)
+        self.handle = C.c_void_p()
+        _check(self.lib.acEnsembleCreate(device_id, len(infos), arr, C.byref(self.handle)),
+               "acEnsembleCreate")
+
+    def destroy(self) -> None:
+        if self.handle:
+            self.lib.acEnsembleDestroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+    def load_member(self, m: int, host: abi.HostMesh) -> None:
+        _check(self.lib.acEnsembleLoadMember(self.handle, m, host.cmesh), "acEnsembleLoadMember")
+
+    def store_member(self, m: int, host: abi.HostMesh) -> None:
+        _check(self.lib.acEnsembleStoreMember(self.handle, m, C.byref(host.cmesh)),
+               "acEnsembleStoreMember")
+
+    def integrate_step(self, dt: float) -> None:
+        _check(self.lib.acEnsembleIntegrateStep(self.handle, dt), "acEnsembleIntegrateStep")
+
+    def integrate_steps(self, dt: float, n: int) -> None:
+        _check(self.lib.acEnsembleIntegrateSteps(self.handle, dt, n), "acEnsembleIntegrateSteps")
+
+    def synchronize(self) -> None:
+        _check(self.lib.acEnsembleSynchronize(self.handle), "acEnsembleSynchronize")
+
+    def status(self) -> int:
+        s = C.c_uint()
+        _check(self.lib.acEnsembleGetStatus(self.handle, C.byref(s)), "acEnsembleGetStatus")
+        return s.value
+
+    def cuda_stream(self) -> int:
+        p = C.c_void_p()
+        _check(self.lib.acEnsembleGetCudaStream(self.handle, C.byref(p)), "acEnsembleGetCudaStream")
+        return p.value or 0
+
+    def launch_count(self) -> int:
+        c = C.c_ulonglong()
+        _check(self.lib.acEnsembleGetLaunchCount(self.handle, C.byref(c)), "acEnsembleGetLaunchCount")
+        return c.value
+
+    def set_schedule(self, config: int, segment_planes: int) -> None:
+        _check(self.lib.acEnsembleSetSchedule(self.handle, config, segment_planes),
+               "acEnsembleSetSchedule")
+
+    def schedule(self) -> tuple[int, int]:
+        c, s = C.c_int(), C.c_int()
+        _check(self.lib.acEnsembleGetSchedule(self.handle, C.byref(c), C.byref(s)),
+               "acEnsembleGetSchedule")
+        return c.value, s.value
+
+    def auto_optimize(self, cache_path: str | None = None) -> None:
+        _check(self.lib.acEnsembleAutoOptimize(self.handle,
+                                               cache_path.encode() if cache_path else None),
+               "acEnsembleAutoOptimize")

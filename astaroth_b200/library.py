@@ -55,6 +55,10 @@ ASTAROTH_B200_H = [
     "acDeviceGetMemoryFootprint", "acDeviceIntegrateStep", "acDeviceIntegrateSteps",
     "acDeviceSetForcing", "acDeviceLoadVertexBufferDouble", "acDeviceStoreVertexBufferDouble",
     "acDeviceReduceScalDouble", "acDeviceReduceVecDouble", "acReduceScalNoAlloc",
+    "acEnsembleCreate", "acEnsembleDestroy", "acEnsembleLoadMember", "acEnsembleStoreMember",
+    "acEnsembleIntegrateStep", "acEnsembleIntegrateSteps", "acEnsembleSynchronize",
+    "acEnsembleGetStatus", "acEnsembleGetCudaStream", "acEnsembleGetLaunchCount",
+    "acEnsembleSetSchedule", "acEnsembleGetSchedule", "acEnsembleAutoOptimize",
 ]
 ALL_SYMBOLS = ASTAROTH_H + ASTAROTH_UTILS_H + ASTAROTH_B200_H
 
@@ -156,6 +160,20 @@ def _declare(lib: C.CDLL, prec: abi.Precision) -> None:
         "acDeviceReduceScalDouble": (res, [Dev, i, i, i, C.POINTER(C.c_double)]),
         "acDeviceReduceVecDouble": (res, [Dev, i, i, i, i, i, C.POINTER(C.c_double)]),
         "acReduceScalNoAlloc": (res, [C.c_void_p, i, C.c_void_p, i, i, i, C.c_void_p]),
+        # ensembles
+        "acEnsembleCreate": (res, [i, i, C.POINTER(Info), C.POINTER(Dev)]),
+        "acEnsembleDestroy": (res, [Dev]),
+        "acEnsembleLoadMember": (res, [Dev, i, Mesh]),
+        "acEnsembleStoreMember": (res, [Dev, i, C.POINTER(Mesh)]),
+        "acEnsembleIntegrateStep": (res, [Dev, R]),
+        "acEnsembleIntegrateSteps": (res, [Dev, R, i]),
+        "acEnsembleSynchronize": (res, [Dev]),
+        "acEnsembleGetStatus": (res, [Dev, C.POINTER(C.c_uint)]),
+        "acEnsembleGetCudaStream": (res, [Dev, C.POINTER(C.c_void_p)]),
+        "acEnsembleGetLaunchCount": (res, [Dev, C.POINTER(C.c_ulonglong)]),
+        "acEnsembleSetSchedule": (res, [Dev, i, i]),
+        "acEnsembleGetSchedule": (res, [Dev, C.POINTER(i), C.POINTER(i)]),
+        "acEnsembleAutoOptimize": (res, [Dev, C.c_char_p]),
     }
     for name, (rt, args) in sig.items():
         fn = getattr(d, name)

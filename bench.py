@@ -11,8 +11,11 @@ FP32 libraries run the same steps beside it for the comparison and the error.
 
 One step = three substeps, each a periodic ghost fill of all fields plus one
 fused solve launch, all through the C ABI (acDevicePeriodicBoundconds,
-acDeviceIntegrateSubstep, acDeviceSwapBuffers). Inputs are larger than L2
-(8.9 GB of state per block), so no L2 flush is needed between steps.
+acDeviceIntegrateSubstep, acDeviceSwapBuffers). A substep over the whole
+interior also stores its results to their periodic ghost images, so after the
+first substep the ghost-fill call finds the ghosts valid and launches nothing.
+Inputs are larger than L2 (8.9 GB of state per block), so no L2 flush is
+needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -52,6 +55,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-variants", action="store_true", help="skip the FP64/FP32 side runs")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-member ensemble")
     return ap.parse_args(argv)
 
 
@@ -329,6 +333,90 @@ def cpu_reference_sample(budget_s: float = 12.0, n: int = 64, max_steps: int | N
             "ms_per_step": 1e3 * tot / len(times), "steps": len(times)}
 
 
+def ensemble_run(steps: int, ranks) -> dict:
+    """The ensemble workload: 64 independent FP32 meshes, 16 each of 32^3,
+    48^3, 96^3 and 128^3, nu and eta log-uniform in [1e-3, 1e-2] per member
+    (seeded), seeded 1e-3 noise. Steps/s of (a) the ensemble, one ghost fill +
+    one solve launch per substep replayed from a CUDA graph, against looping
+    single-mesh Devices (b) launching asynchronously (each Device on its own
+    streams, so the GPU overlaps members) and (c) synchronising each member's
+    step as the reference's Node/Legacy integrate does."""
+    import numpy as np
+    import torch
+
+    from astaroth_b200 import Device, Ensemble, abi, init
+
+    prec = abi.SP
+    sizes = [32] * 16 + [48] * 16 + [96] * 16 + [128] * 16
+    rng = np.random.default_rng(2024)
+    infos, hosts = [], []
+    for k, n in enumerate(sizes):
+        nu, eta = 10 ** rng.uniform(-3, -2, 2)
+        ds = 2 * math.pi / n
+        info = abi.make_info(prec, n, dsx=ds, dsy=ds, dsz=ds, gamma=5 / 3, cs_sound=1.0,
+                             cp_sound=1.0, nu_visc=nu, eta=eta)
+        h = abi.HostMesh(prec, info)
+        gen = init.workload_fields_torch(n, n, n, torch.float32, seed=100 + k, amplitude=1e-3,
+                                         device="cuda")
+        for w, g in enumerate(gen):
+            h.fields[w][...] = g.cpu().numpy()
+        infos.append(info)
+        hosts.append(h)
+    cells = sum(n ** 3 for n in sizes)
+    dev_index = torch.cuda.current_device()
+
+    ens = Ensemble("sp", infos, dev_index)
+    for k in range(len(sizes)):
+        ens.load_member(k, hosts[k])
+    ens.auto_optimize()
+    st = torch.cuda.ExternalStream(ens.cuda_stream())
+    ens.integrate_steps(DT, 2)
+    ens.synchronize()
+    ranks.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ens.launch_count()
+    e0.record(st)
+    ens.integrate_steps(DT, steps)
+    e1.record(st)
+    e1.synchronize()
+    ens_ms = ranks.max(e0.elapsed_time(e1) / steps)
+    ens_launches = ens.launch_count() - l0
+    cfg, seg = ens.schedule()
+    ens.destroy()
+
+    devs = [Device("sp", infos[k], dev_index) for k in range(len(sizes))]
+    for k, d in enumerate(devs):
+        d.load_mesh(hosts[k])
+
+    def loop(sync_each: bool) -> float:
+        for d in devs:
+            d.integrate_step(DT)
+        torch.cuda.synchronize()
+        ranks.barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            for d in devs:
+                d.integrate_step(DT)
+                if sync_each:
+                    d.synchronize(0)
+        torch.cuda.synchronize()
+        return ranks.max((time.perf_counter() - t0) * 1e3 / steps)
+
+    loop_async = loop(False)
+    loop_sync = loop(True)
+    for d in devs:
+        d.destroy()
+    return {"members": "16 x 32^3, 16 x 48^3, 16 x 96^3, 16 x 128^3 (FP32)",
+            "cells": cells, "ensemble_ms_per_step": ens_ms,
+            "ensemble_steps_per_s": 1e3 / ens_ms,
+            "ensemble_cell_updates_per_s": ranks.world * cells / (ens_ms * 1e-3),
+            "ensemble_launches_per_step": ens_launches / steps,
+            "schedule": {"tile_config": cfg, "segment_planes": seg},
+            "loop_async_ms_per_step": loop_async, "loop_sync_ms_per_step": loop_sync,
+            "speedup_vs_loop_async": loop_async / ens_ms,
+            "speedup_vs_loop_sync": loop_sync / ens_ms}
+
+
 def profile_traffic(name: str):
     """Per-launch DRAM bytes of the dominant kernel from a committed ncu
     summary (a line `traffic_bytes_per_launch: <value>`), else None."""
@@ -444,6 +532,10 @@ def run_ours(args) -> None:
                "includes": "mesh load from pinned host, per-step max|u| read back, mesh store"}
         del h
 
+    ensemble = None
+    if not args.no_ensemble:
+        ensemble = ensemble_run(min(args.steps, 20), ranks)
+
     cpu = None
     if ranks.rank == 0 and not args.no_cpu:
         c = cpu_reference_sample(budget_s=12.0)
@@ -462,7 +554,8 @@ def run_ours(args) -> None:
                              "alg_bytes_per_cell_step": alg // n ** 3,
                              "solve_ms_per_substep": res["solve_ms_per_substep"]},
                 "clocks": res["clocks"], "gpu_launches": res["launches"],
-                "e2e": e2e, "cpu_baseline": cpu, "variants": variants, "errors": errors}
+                "e2e": e2e, "cpu_baseline": cpu, "variants": variants, "errors": errors,
+                "ensemble": ensemble}
         print(json.dumps(line), flush=True)
     ranks.close()
 

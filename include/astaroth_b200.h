@@ -56,6 +56,40 @@ AcResult acDeviceIntegrateSteps(const Device device, const Stream stream, const 
  * AC_ff_hel_* / AC_kaver uniforms. */
 AcResult acDeviceSetForcing(const Device device, const int enabled);
 
+/* ---- ensembles ------------------------------------------------------------
+ * Many independent meshes (members) of possibly different sizes and
+ * parameters on one GPU, advanced together: each substep is ONE ghost-fill
+ * launch and ONE persistent solve launch over the tiles of all members, and
+ * whole steps replay from a captured CUDA graph. Each member's AcMeshInfo
+ * supplies its size and physics (AC_nu_visc, AC_eta, ...); dt is common. */
+typedef struct ensemble_s* Ensemble;
+
+AcResult acEnsembleCreate(const int device_id, const int num_members, const AcMeshInfo* configs,
+                          Ensemble* ensemble);
+AcResult acEnsembleDestroy(Ensemble ensemble);
+/* Whole-mesh transfers of one member (mx*my*mz per field, reference order). */
+AcResult acEnsembleLoadMember(Ensemble ensemble, const int member, const AcMesh host_mesh);
+AcResult acEnsembleStoreMember(Ensemble ensemble, const int member, AcMesh* host_mesh);
+/* One RK3 step of every member: 3 x (batched ghost fill, batched substep,
+ * swap). Asynchronous on the ensemble's stream. */
+AcResult acEnsembleIntegrateStep(Ensemble ensemble, const AcReal dt);
+/* num_steps steps replayed from a captured graph (one per buffer parity). */
+AcResult acEnsembleIntegrateSteps(Ensemble ensemble, const AcReal dt, const int num_steps);
+AcResult acEnsembleSynchronize(Ensemble ensemble);
+AcResult acEnsembleGetStatus(Ensemble ensemble, unsigned* status);
+AcResult acEnsembleGetCudaStream(Ensemble ensemble, void** cuda_stream);
+AcResult acEnsembleGetLaunchCount(Ensemble ensemble, unsigned long long* count);
+/* Schedule: tile configuration (index into the compiled table) and the target
+ * number of planes per z segment of a task (0 = whole columns). */
+AcResult acEnsembleSetSchedule(Ensemble ensemble, const int config, const int segment_planes);
+AcResult acEnsembleGetSchedule(Ensemble ensemble, int* config, int* segment_planes);
+/* Times every (configuration, segment length) pair on this ensemble and keeps
+ * the fastest; results are cached in a text file keyed by the precision and
+ * the member sizes (cache_path NULL: $ACB_TUNE_CACHE, else
+ * ~/.cache/astaroth_b200/tune.txt). Only the scratch `out` buffers are
+ * touched, so the members' states are preserved between whole steps. */
+AcResult acEnsembleAutoOptimize(Ensemble ensemble, const char* cache_path);
+
 /* ---- double-precision views (useful in every build; exact in dp) --------- */
 
 /* Loads / stores one whole field (mx*my*mz values, reference index order)

@@ -360,3 +360,30 @@ def test_reference_ctest_sample_runs(tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     assert "ctest complete." in r.stdout
     assert "FAIL" not in r.stdout
+
+
+@pytest.mark.parametrize("flavour", FLAVOURS)
+@pytest.mark.parametrize("dims", [(20, 14, 11), (131, 5, 4), (7, 4, 5)])
+def test_whole_box_fill_after_substep_is_exact(flavour, dims):
+    """The whole-box ghost fill (interior-row x-ghosts and ghost rows as
+    separate work units, rows wider than one 128-vertex chunk included) must
+    leave every ghost equal to its periodic image of the interior that the
+    substep just wrote; a second fill of the same block is skipped and must
+    change nothing."""
+    prec = abi.PRECISIONS[flavour]
+    nx, ny, nz = dims
+    info = workload_info(prec, nx, ny, nz)
+    fields = init.workload_fields(nx, ny, nz, prec.np_dtype, seed=13, amplitude=0.05)
+    host = abi.HostMesh(prec, info, fields)
+    with new_device(flavour, info) as dev:
+        dev.load_mesh(host)
+        dev.periodic_boundconds()
+        dev.integrate_substep(0, 1e-3)
+        dev.swap_buffers()
+        dev.periodic_boundconds()
+        first = [dev.store_double(w) for w in range(8)]
+        dev.periodic_boundconds()
+        second = [dev.store_double(w) for w in range(8)]
+    for w in range(8):
+        assert np.array_equal(first[w], init.wrap_ghosts(interior(first[w]))), w
+        assert np.array_equal(first[w], second[w]), w
