@@ -175,10 +175,24 @@ AcResult
 acb_host::prepare_table(const SolveConfig* cfgs, int n)
 {
     for (int c = 0; c < n; ++c)
-        for (int st = 0; st < 3; ++st)
+        for (int st = 0; st < 4; ++st) {
+            if (!cfgs[c].kern[st])
+                continue;
             ACB_CUDA_CHECK(cudaFuncSetAttribute((const void*)cfgs[c].kern[st],
                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int)cfgs[c].smem));
+            // kernels that move registers between warpgroups must start with
+            // enough of them, or the consumers' increase would wait for ever
+            cudaFuncAttributes fa;
+            ACB_CUDA_CHECK(cudaFuncGetAttributes(&fa, (const void*)cfgs[c].kern[st]));
+            if (fa.numRegs < cfgs[c].launch_regs) {
+                fprintf(stderr,
+                        "astaroth_b200: solve kernel %s built with %d registers a thread, "
+                        "needs %d for its register reallocation; refusing to launch it\n",
+                        cfgs[c].name, fa.numRegs, cfgs[c].launch_regs);
+                return AC_FAILURE;
+            }
+        }
     return AC_SUCCESS;
 }
 
@@ -334,8 +348,9 @@ launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e)
     a.status     = d->status;
     a.P          = make_params(d->uniforms, d->L, step, d->forcing);
 
+    const SolveKernelFn kern = cfg.kern[step == 2 && d->forcing ? 3 : step];
     int per_sm = 0;
-    ACB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.kern[step],
+    ACB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern,
                                                                  cfg.threads, cfg.smem));
     if (per_sm < 1)
         per_sm = 1;
@@ -347,7 +362,7 @@ launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e)
     g.nseg  = (g.nzr + g.zseg - 1) / g.zseg;
     g.tasks = ntiles * g.nseg;
     long long grid = std::min(slots, g.tasks);
-    cfg.kern[step]<<<(unsigned)grid, cfg.threads, cfg.smem, st>>>(d->tmap[d->cur], a);
+    kern<<<(unsigned)grid, cfg.threads, cfg.smem, st>>>(d->tmap[d->cur], a);
     ACB_CUDA_CHECK(cudaGetLastError());
     d->launches++;
     d->ghost_ok[d->cur ^ 1] = false; // the out block's ghosts are stale now

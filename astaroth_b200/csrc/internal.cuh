@@ -23,8 +23,9 @@ typedef void (*SolveKernelFn)(const CUtensorMap, const SolveArgs<AcReal>);
 struct SolveConfig {
     const char* name;
     int TX, TY, NP, threads;
+    int launch_regs; // registers a thread the kernels must be launched with (0: any)
     size_t smem;
-    SolveKernelFn kern[3]; // substeps 0, 1, 2
+    SolveKernelFn kern[4]; // substeps 0, 1, 2, and 2 with helical forcing (single mesh only)
 };
 
 template <class Cfg, bool ENS>
@@ -37,10 +38,15 @@ make_solve_config(const char* name)
     c.TY      = Cfg::TY;
     c.NP      = Cfg::NP;
     c.threads = Cfg::THREADS;
+    c.launch_regs = Cfg::REG_LAUNCH;
     c.smem    = Cfg::smem_bytes();
     c.kern[0] = solve_kernel<Cfg, 0, ENS>;
     c.kern[1] = solve_kernel<Cfg, 1, ENS>;
     c.kern[2] = solve_kernel<Cfg, 2, ENS>;
+    if constexpr (ENS)
+        c.kern[3] = nullptr;
+    else
+        c.kern[3] = solve_kernel<Cfg, 3, ENS>;
     return c;
 }
 

@@ -10,6 +10,7 @@
 //   state" form:  s = 0   : out = in + beta1 * dt * f
 //                 s = 1, 2: out = in + beta_{s+1} (alpha_{s+1}/beta_s (in - out) + dt f)
 //   forcing (s = 2 only)   acc/mhd_solver/stencil_kernel.ac:611-648,713-717
+//                          (STEP 3 = substep 2 with forcing; STEP 2 leaves it out)
 //
 // B200 structure (no counterpart in the reference, which reads 55 stencil points
 // per field straight from global memory with one thread per vertex):
@@ -21,9 +22,14 @@
 //     into a ring of NP plane slots in shared memory (mbarrier `full` with
 //     transaction bytes); consumer warps release a slot through an `empty`
 //     mbarrier when done, so no block-wide barrier sits in the plane loop;
-//   - one consumer thread per (x, y) column; every stencil operand, including
-//     the z-neighbours and the xz/yz diagonals, is read from the ring; the
-//     centre-only values (previous state, lo parts) are loaded a plane ahead;
+//   - one consumer thread per (x, y) column; in single precision each thread
+//     keeps a register queue along z (its column's values of the three planes
+//     below, and the x / y differences the xz / yz diagonals need from them),
+//     so the ring is read for the centre plane and the three above it only
+//     (224 instead of 296 shared-memory reads per vertex) and a plane's slot is
+//     released as soon as its own outputs are done; double precision reads all
+//     seven planes from the ring; the centre-only values (previous state, lo
+//     parts) are loaded from global memory at the top of each plane;
 //   - derivative coefficients arrive pre-scaled by 1/ds (and 1/ds^2) so each
 //     pencil costs 6-7 FP ops; only the 21 first, 24 second and 12 cross
 //     derivatives the right-hand sides use are formed;
@@ -92,7 +98,17 @@ struct TileCfg {
     static constexpr int BX = TX_ + 8, BY = TY_ + 6;
     static constexpr int CONSUMERS = TX_ * TY_;        // one thread per (x, y) column
     static constexpr int CWARPS    = CONSUMERS / 32;   // consumer warps
-    static constexpr int THREADS   = CONSUMERS + 32;   // plus one producer warp
+    // Single precision with 8 consumer warps: the producer is a whole
+    // warpgroup (4 warps, one of them working) that hands its registers to the
+    // consumers (setmaxnreg), so each consumer thread gets 232 registers for
+    // its z queues. An SM sub-partition's 16K registers hold 2 consumer warps
+    // and 1 producer warp: 2 * 232 + 40 = 504 <= 512 registers a lane.
+    static constexpr bool WGSPEC   = sizeof(state_t) == 4 && CWARPS == 8;
+    static constexpr int THREADS   = CONSUMERS + (WGSPEC ? 128 : 32); // plus the producer
+    static constexpr int REG_CONSUMER = 232, REG_PRODUCER = 40;
+    // registers a thread the launch must hold for the reallocation to balance
+    static constexpr int REG_LAUNCH =
+        WGSPEC ? (REG_CONSUMER * CONSUMERS + REG_PRODUCER * 128 + THREADS - 1) / THREADS : 0;
     static constexpr int FIELD   = BX * BY;
     static constexpr int PLANE   = ACB_NF * FIELD; // elements per ring slot
     static constexpr size_t smem_bytes() { return (size_t)NP * PLANE * sizeof(state_t); }
@@ -111,6 +127,20 @@ __device__ __forceinline__ float
 rexp<float>(float x)
 {
     return expf(x);
+}
+
+// 1 / x, correctly rounded (the same value as the IEEE division)
+template <typename T>
+__device__ __forceinline__ T
+rrcp(T x)
+{
+    return __drcp_rn(x);
+}
+template <>
+__device__ __forceinline__ float
+rrcp<float>(float x)
+{
+    return __frcp_rn(x);
 }
 
 // first and second derivative from the six neighbours of a pencil
@@ -207,24 +237,214 @@ field_derivs(const state_t* __restrict__ c, const int* zo, const SolveParams<T>&
     return r;
 }
 
-// Right-hand sides of the eight fields at one vertex (stencil_kernel.ac:355-528,
-// restated; same terms, evaluated from the derivative set above).
+// Register queue of one field along z (2.5D streaming): the values of the
+// thread's own column at the three planes below the current one, and, for a
+// field with an xz (yz) cross derivative, the x (y) differences
+// d_k = f(+k) - f(-k) of those planes. The diagonal cross derivative
+//   sum_k e_k (f(+k,+k) + f(-k,-k) - f(+k,-k) - f(-k,+k))
+// equals sum_k e_k (d_k(z+k) - d_k(z-k)), so its lower half comes from the
+// queue and only the upper half is read from the ring; likewise the lower
+// half of the z pencil.
+template <typename T>
+struct ZQueue {
+    T v1, v2, v3;                  // f at z-1, z-2, z-3
+    T x1, x2a, x2b, x3a, x3b, x3c; // dx_1(z-1); dx_2(z-1), dx_2(z-2); dx_3(z-1), (z-2), (z-3)
+    T y1, y2a, y2b, y3a, y3b, y3c; // the same for dy
+};
+
+// Fills the queue from the ring at the first plane of a task (zo[0..2]: the
+// three planes below it).
+template <typename T, int BX, bool XZ, bool YZ>
+__device__ __forceinline__ void
+prime_queue(const state_t* __restrict__ c, const int* zo, ZQueue<T>& Q)
+{
+    Q.v1 = c[zo[2]];
+    Q.v2 = c[zo[1]];
+    Q.v3 = c[zo[0]];
+    if (XZ) {
+        Q.x1  = (T)c[zo[2] + 1] - (T)c[zo[2] - 1];
+        Q.x2a = (T)c[zo[2] + 2] - (T)c[zo[2] - 2];
+        Q.x2b = (T)c[zo[1] + 2] - (T)c[zo[1] - 2];
+        Q.x3a = (T)c[zo[2] + 3] - (T)c[zo[2] - 3];
+        Q.x3b = (T)c[zo[1] + 3] - (T)c[zo[1] - 3];
+        Q.x3c = (T)c[zo[0] + 3] - (T)c[zo[0] - 3];
+    }
+    if (YZ) {
+        Q.y1  = (T)c[zo[2] + BX] - (T)c[zo[2] - BX];
+        Q.y2a = (T)c[zo[2] + 2 * BX] - (T)c[zo[2] - 2 * BX];
+        Q.y2b = (T)c[zo[1] + 2 * BX] - (T)c[zo[1] - 2 * BX];
+        Q.y3a = (T)c[zo[2] + 3 * BX] - (T)c[zo[2] - 3 * BX];
+        Q.y3b = (T)c[zo[1] + 3 * BX] - (T)c[zo[1] - 3 * BX];
+        Q.y3c = (T)c[zo[0] + 3 * BX] - (T)c[zo[0] - 3 * BX];
+    }
+}
+
+// field_derivs with the lower z half from the queue; advances the queue by one
+// plane. Ring reads: x and y pencils (12), centre (1), upper z half (3), upper
+// halves of the xz / yz diagonals (6 each) and the whole xy diagonal (12),
+// i.e. 16 + 6 * (XZ + YZ) + 12 * XY instead of 19 + 12 * (XY + XZ + YZ).
+template <typename T, int BX, bool GX, bool GY, bool GZ, bool XY, bool XZ, bool YZ>
+__device__ __forceinline__ FieldDerivs<T>
+field_derivs_q(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, ZQueue<T>& Q)
+{
+    FieldDerivs<T> r;
+    const T f0 = (T)c[0];
+    r.v        = f0;
+    T dx1, dx2, dx3, dy1, dy2, dy3;
+    // x pencil
+    {
+        const T m1 = c[-1], p1 = c[1], m2 = c[-2], p2 = c[2], m3 = c[-3], p3 = c[3];
+        dx1 = p1 - m1;
+        dx2 = p2 - m2;
+        dx3 = p3 - m3;
+        if (GX)
+            r.gx = P.c1[0][0] * dx1 + P.c1[0][1] * dx2 + P.c1[0][2] * dx3;
+        r.xx = dd2(f0, m1, p1, m2, p2, m3, p3, P.c2[0]);
+    }
+    // y pencil
+    {
+        const T m1 = c[-BX], p1 = c[BX], m2 = c[-2 * BX], p2 = c[2 * BX], m3 = c[-3 * BX],
+                p3 = c[3 * BX];
+        dy1 = p1 - m1;
+        dy2 = p2 - m2;
+        dy3 = p3 - m3;
+        if (GY)
+            r.gy = P.c1[1][0] * dy1 + P.c1[1][1] * dy2 + P.c1[1][2] * dy3;
+        r.yy = dd2(f0, m1, p1, m2, p2, m3, p3, P.c2[1]);
+    }
+    // z pencil: lower half from the queue
+    {
+        const T m1 = Q.v1, m2 = Q.v2, m3 = Q.v3;
+        const T p1 = c[zo[4]], p2 = c[zo[5]], p3 = c[zo[6]];
+        if (GZ)
+            d12(f0, m1, p1, m2, p2, m3, p3, P.c1[2], P.c2[2], r.gz, r.zz);
+        else
+            r.zz = dd2(f0, m1, p1, m2, p2, m3, p3, P.c2[2]);
+    }
+    if (XY) {
+        T s = 0;
+#pragma unroll
+        for (int k = 1; k <= 3; ++k) {
+            const T a = (T)c[k + k * BX] + (T)c[-k - k * BX];
+            const T b = (T)c[k - k * BX] + (T)c[-k + k * BX];
+            s += P.cx[0][k - 1] * (a - b);
+        }
+        r.xy = s;
+    }
+    if (XZ) {
+        const T u1 = (T)c[zo[4] + 1] - (T)c[zo[4] - 1];
+        const T u2 = (T)c[zo[5] + 2] - (T)c[zo[5] - 2];
+        const T u3 = (T)c[zo[6] + 3] - (T)c[zo[6] - 3];
+        T s = P.cx[1][0] * (u1 - Q.x1);
+        s += P.cx[1][1] * (u2 - Q.x2b);
+        s += P.cx[1][2] * (u3 - Q.x3c);
+        r.xz  = s;
+        Q.x3c = Q.x3b;
+        Q.x3b = Q.x3a;
+        Q.x3a = dx3;
+        Q.x2b = Q.x2a;
+        Q.x2a = dx2;
+        Q.x1  = dx1;
+    }
+    if (YZ) {
+        const T u1 = (T)c[zo[4] + BX] - (T)c[zo[4] - BX];
+        const T u2 = (T)c[zo[5] + 2 * BX] - (T)c[zo[5] - 2 * BX];
+        const T u3 = (T)c[zo[6] + 3 * BX] - (T)c[zo[6] - 3 * BX];
+        T s = P.cx[2][0] * (u1 - Q.y1);
+        s += P.cx[2][1] * (u2 - Q.y2b);
+        s += P.cx[2][2] * (u3 - Q.y3c);
+        r.yz  = s;
+        Q.y3c = Q.y3b;
+        Q.y3b = Q.y3a;
+        Q.y3a = dy3;
+        Q.y2b = Q.y2a;
+        Q.y2a = dy2;
+        Q.y1  = dy1;
+    }
+    Q.v3 = Q.v2;
+    Q.v2 = Q.v1;
+    Q.v1 = f0;
+    return r;
+}
+
+// Derivative flags of the eight fields: what the right-hand sides use.
+//                   GX     GY     GZ     XY     XZ     YZ
+#define ACB_D_LNRHO true, true, true, false, false, false
+#define ACB_D_UUX true, true, true, true, true, false
+#define ACB_D_UUY true, true, true, true, false, true
+#define ACB_D_UUZ true, true, true, false, true, true
+#define ACB_D_AX false, true, true, true, true, false
+#define ACB_D_AY true, false, true, true, false, true
+#define ACB_D_AZ true, true, false, false, true, true
+#define ACB_D_SS true, true, true, false, false, false
+
+template <typename T>
+__device__ __forceinline__ void rhs_terms(const FieldDerivs<T>& lr, const FieldDerivs<T>& ux,
+                                          const FieldDerivs<T>& uy, const FieldDerivs<T>& uz,
+                                          const FieldDerivs<T>& ax, const FieldDerivs<T>& ay,
+                                          const FieldDerivs<T>& az, const FieldDerivs<T>& ss,
+                                          const SolveParams<T>& P, T roc[ACB_NF], T cur[ACB_NF]);
+
+// Right-hand sides of the eight fields at one vertex, every stencil operand
+// read from the ring.
 template <typename T, int BX, int FIELD>
 __device__ __forceinline__ void
 mhd_rhs(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, T roc[ACB_NF],
         T cur[ACB_NF])
 {
-    //                                       GX     GY     GZ     XY     XZ     YZ
-    const auto lr = field_derivs<T, BX, true, true, true, false, false, false>(c + 0 * FIELD, zo, P);
-    const auto ux = field_derivs<T, BX, true, true, true, true, true, false>(c + 1 * FIELD, zo, P);
-    const auto uy = field_derivs<T, BX, true, true, true, true, false, true>(c + 2 * FIELD, zo, P);
-    const auto uz = field_derivs<T, BX, true, true, true, false, true, true>(c + 3 * FIELD, zo, P);
-    const auto ax = field_derivs<T, BX, false, true, true, true, true, false>(c + 4 * FIELD, zo, P);
-    const auto ay = field_derivs<T, BX, true, false, true, true, false, true>(c + 5 * FIELD, zo, P);
-    const auto az = field_derivs<T, BX, true, true, false, false, true, true>(c + 6 * FIELD, zo, P);
-    const auto ss = field_derivs<T, BX, true, true, true, false, false, false>(c + 7 * FIELD, zo, P);
+    const auto lr = field_derivs<T, BX, ACB_D_LNRHO>(c + 0 * FIELD, zo, P);
+    const auto ux = field_derivs<T, BX, ACB_D_UUX>(c + 1 * FIELD, zo, P);
+    const auto uy = field_derivs<T, BX, ACB_D_UUY>(c + 2 * FIELD, zo, P);
+    const auto uz = field_derivs<T, BX, ACB_D_UUZ>(c + 3 * FIELD, zo, P);
+    const auto ax = field_derivs<T, BX, ACB_D_AX>(c + 4 * FIELD, zo, P);
+    const auto ay = field_derivs<T, BX, ACB_D_AY>(c + 5 * FIELD, zo, P);
+    const auto az = field_derivs<T, BX, ACB_D_AZ>(c + 6 * FIELD, zo, P);
+    const auto ss = field_derivs<T, BX, ACB_D_SS>(c + 7 * FIELD, zo, P);
+    rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
+}
 
+// The same with the z register queues.
+template <typename T, int BX, int FIELD>
+__device__ __forceinline__ void
+mhd_rhs_q(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, T roc[ACB_NF],
+          T cur[ACB_NF], ZQueue<T> (&Q)[ACB_NF])
+{
+    const auto lr = field_derivs_q<T, BX, ACB_D_LNRHO>(c + 0 * FIELD, zo, P, Q[0]);
+    const auto ux = field_derivs_q<T, BX, ACB_D_UUX>(c + 1 * FIELD, zo, P, Q[1]);
+    const auto uy = field_derivs_q<T, BX, ACB_D_UUY>(c + 2 * FIELD, zo, P, Q[2]);
+    const auto uz = field_derivs_q<T, BX, ACB_D_UUZ>(c + 3 * FIELD, zo, P, Q[3]);
+    const auto ax = field_derivs_q<T, BX, ACB_D_AX>(c + 4 * FIELD, zo, P, Q[4]);
+    const auto ay = field_derivs_q<T, BX, ACB_D_AY>(c + 5 * FIELD, zo, P, Q[5]);
+    const auto az = field_derivs_q<T, BX, ACB_D_AZ>(c + 6 * FIELD, zo, P, Q[6]);
+    const auto ss = field_derivs_q<T, BX, ACB_D_SS>(c + 7 * FIELD, zo, P, Q[7]);
+    rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
+}
+
+template <typename T, int BX, int FIELD>
+__device__ __forceinline__ void
+prime_queues(const state_t* __restrict__ c, const int* zo, ZQueue<T> (&Q)[ACB_NF])
+{
+    prime_queue<T, BX, false, false>(c + 0 * FIELD, zo, Q[0]);
+    prime_queue<T, BX, true, false>(c + 1 * FIELD, zo, Q[1]);
+    prime_queue<T, BX, false, true>(c + 2 * FIELD, zo, Q[2]);
+    prime_queue<T, BX, true, true>(c + 3 * FIELD, zo, Q[3]);
+    prime_queue<T, BX, true, false>(c + 4 * FIELD, zo, Q[4]);
+    prime_queue<T, BX, false, true>(c + 5 * FIELD, zo, Q[5]);
+    prime_queue<T, BX, true, true>(c + 6 * FIELD, zo, Q[6]);
+    prime_queue<T, BX, false, false>(c + 7 * FIELD, zo, Q[7]);
+}
+
+// Right-hand sides from the derivative sets (stencil_kernel.ac:355-528,
+// restated; same terms).
+template <typename T>
+__device__ __forceinline__ void
+rhs_terms(const FieldDerivs<T>& lr, const FieldDerivs<T>& ux, const FieldDerivs<T>& uy,
+          const FieldDerivs<T>& uz, const FieldDerivs<T>& ax, const FieldDerivs<T>& ay,
+          const FieldDerivs<T>& az, const FieldDerivs<T>& ss, const SolveParams<T>& P,
+          T roc[ACB_NF], T cur[ACB_NF])
+{
     cur[0] = lr.v;
+
     cur[1] = ux.v;
     cur[2] = uy.v;
     cur[3] = uz.v;
@@ -271,7 +491,7 @@ mhd_rhs(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, T
     const T expE    = rexp<T>(E);
     const T cs2     = P.cs2_sound * expE;
     const T rho     = rexp<T>(lr.v);
-    const T inv_rho = (T)1 / rho;
+    const T inv_rho = rrcp<T>(rho);
 
     // momentum
     const T gd0 = ux.xx + uy.xy + uz.xz;
@@ -295,7 +515,7 @@ mhd_rhs(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, T
 
     // entropy
     const T lnT    = P.lnT0 + E;
-    const T inv_pT = (T)1 / (rho * rexp<T>(lnT));
+    const T inv_pT = rrcp<T>(rho * rexp<T>(lnT));
     const T SS     = S00 * S00 + S01 * S01 + S02 * S02 + S01 * S01 + S11 * S11 + S12 * S12 +
                  S02 * S02 + S12 * S12 + S22 * S22;
     const T heat = P.eta_mu0 * (j0 * j0 + j1 * j1 + j2 * j2) + (T)2 * rho * P.nu * SS +
@@ -452,9 +672,27 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
         ok = mbar_wait_bounded(&full[(q + l) % NP], ((q + l) / NP) & 1u);
     ok = __all_sync(0xffffffffu, ok);
 
-    CentreVals cv;
-    if (act)
-        load_centre<STEP>(L, out, in_lo, out_lo, lidx(L, i, j, tg.k0), cv);
+    // single precision streams with the z register queues (2.5D); double
+    // precision has no registers to spare for them and reads every operand
+    // from the ring
+    constexpr bool QZ = sizeof(state_t) == 4;
+    acb::ZQueue<T> Q[ACB_NF];
+    if constexpr (QZ) {
+        if (ok && act) {
+            const uint32_t sc = (q + NGHOST) % NP;
+            int zo[7];
+#pragma unroll
+            for (int dz = -NGHOST; dz <= NGHOST; ++dz)
+                zo[dz + NGHOST] = ((int)((q + NGHOST + dz) % NP) - (int)sc) * PLANE;
+            const state_t* c = ring + (size_t)sc * PLANE + (ty + NGHOST) * BX + (tx + 4);
+            acb::prime_queues<T, BX, FIELD>(c, zo, Q);
+        }
+        // the three planes below the first output plane now live in the queues
+        __syncwarp();
+        if (lane == 0 && ok)
+            for (int l = 0; l < NGHOST; ++l)
+                mbar_arrive(&empty[(q + l) % NP]);
+    }
 
     for (int p = 0; p < tg.nout; ++p) {
         if (ok) {
@@ -470,25 +708,31 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
             return false;
         }
         const int k = tg.k0 + p;
-        CentreVals nx_cv; // next plane's centre values, loaded a plane ahead
-        if (act && p + 1 < tg.nout)
-            load_centre<STEP>(L, out, in_lo, out_lo, lidx(L, i, j, k + 1), nx_cv);
         if (act) {
+            const long long id = lidx(L, i, j, k);
+            // previous state and lo parts of this vertex: issued first, used
+            // only by the update at the end of the plane
+            CentreVals cv;
+            load_centre<STEP>(L, out, in_lo, out_lo, id, cv);
             const uint32_t sc = (q + p + NGHOST) % NP;
             int zo[7];
 #pragma unroll
             for (int dz = -NGHOST; dz <= NGHOST; ++dz) {
+                if (QZ && dz < 0)
+                    continue;
                 const int sd    = (int)((q + p + NGHOST + dz) % NP);
                 zo[dz + NGHOST] = (sd - (int)sc) * PLANE;
             }
             const state_t* c = ring + (size_t)sc * PLANE + (ty + NGHOST) * BX + (tx + 4);
-            const long long id = lidx(L, i, j, k);
 
             T roc[ACB_NF], cur[ACB_NF];
-            acb::mhd_rhs<T, BX, FIELD>(c, zo, P, roc, cur);
+            if constexpr (QZ)
+                acb::mhd_rhs_q<T, BX, FIELD>(c, zo, P, roc, cur, Q);
+            else
+                acb::mhd_rhs<T, BX, FIELD>(c, zo, P, roc, cur);
 
             T fo[3] = {0, 0, 0};
-            if (!ENS && STEP == 2 && a.P.forcing)
+            if constexpr (STEP == 3)
                 acb::forcing_at<T>(a.P, i, j, k, fo);
 
 #pragma unroll
@@ -499,7 +743,7 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
                     d += rkA * ((cur[f] - cv.prev[f]) + (cv.cur_lo[f] - cv.prev_lo[f]));
                 float hi, lo;
                 acb::pair_add(cur[f], cv.cur_lo[f], d, hi, lo);
-                if (STEP == 2 && f >= 1 && f <= 3)
+                if (STEP == 3 && f >= 1 && f <= 3)
                     acb::pair_add(hi, lo, fo[f - 1], hi, lo);
                 out[f * L.fstride + id]    = hi;
                 out_lo[f * L.fstride + id] = lo;
@@ -509,21 +753,22 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
                     r = cur[f] + rkB * roc[f];
                 else
                     r = cur[f] + rkA * (cur[f] - cv.prev[f]) + rkB * roc[f];
-                if (STEP == 2 && f >= 1 && f <= 3)
+                if (STEP == 3 && f >= 1 && f <= 3)
                     r += fo[f - 1];
                 out[f * L.fstride + id] = r;
 #endif
             }
         }
-        cv = nx_cv;
         __syncwarp();
+        // with the queues the centre plane is done with; without them the
+        // plane three below it
         if (lane == 0)
-            mbar_arrive(&empty[(q + p) % NP]); // this warp is done with plane p
+            mbar_arrive(&empty[(q + p + (QZ ? NGHOST : 0)) % NP]);
     }
-    // the task's last six planes are no longer needed either
+    // the planes of the task not released yet
     __syncwarp();
     if (lane == 0)
-        for (int l = tg.nout; l < nload; ++l)
+        for (int l = tg.nout + (QZ ? NGHOST : 0); l < nload; ++l)
             mbar_arrive(&empty[(q + l) % NP]);
     q += nload;
     return true;
@@ -570,9 +815,17 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
 
     const long long ntasks = ENS ? a.total_tasks : a.g.tasks;
 
-    if (warp == CWARPS) {
+    if constexpr (Cfg::WGSPEC) {
+        // whole warpgroups: warps 0..7 consume, warps 8..11 produce
+        if (warp >= CWARPS)
+            asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(Cfg::REG_PRODUCER));
+        else
+            asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(Cfg::REG_CONSUMER));
+    }
+
+    if (warp >= CWARPS) {
         // ------------------------------------------------------------ producer
-        if (lane == 0) {
+        if (warp == CWARPS && lane == 0) {
             if (!ENS)
                 prefetch_tensormap(&tin);
             uint32_t q  = 0;
