@@ -29,7 +29,8 @@
 //     (224 instead of 296 shared-memory reads per vertex) and a plane's slot is
 //     released as soon as its own outputs are done; double precision reads all
 //     seven planes from the ring; the centre-only values (previous state, lo
-//     parts) are loaded from global memory at the top of each plane;
+//     parts) are loaded from global memory at the top of each plane (a plane
+//     ahead in double precision);
 //   - derivative coefficients arrive pre-scaled by 1/ds (and 1/ds^2) so each
 //     pencil costs 6-7 FP ops; only the 21 first, 24 second and 12 cross
 //     derivatives the right-hand sides use are formed;
@@ -694,6 +695,13 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
                 mbar_arrive(&empty[(q + l) % NP]);
     }
 
+    // double precision (no queues, registers to spare for it): the centre
+    // values of the next plane are loaded a plane ahead
+    constexpr bool PREF = !QZ;
+    CentreVals cv_next;
+    if (PREF && act)
+        load_centre<STEP>(L, out, in_lo, out_lo, lidx(L, i, j, tg.k0), cv_next);
+
     for (int p = 0; p < tg.nout; ++p) {
         if (ok) {
             const uint32_t l = q + p + 2 * NGHOST;
@@ -713,7 +721,14 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
             // previous state and lo parts of this vertex: issued first, used
             // only by the update at the end of the plane
             CentreVals cv;
-            load_centre<STEP>(L, out, in_lo, out_lo, id, cv);
+            if constexpr (PREF) {
+                cv = cv_next;
+                if (p + 1 < tg.nout)
+                    load_centre<STEP>(L, out, in_lo, out_lo, id + L.plane, cv_next);
+            }
+            else {
+                load_centre<STEP>(L, out, in_lo, out_lo, id, cv);
+            }
             const uint32_t sc = (q + p + NGHOST) % NP;
             int zo[7];
 #pragma unroll
