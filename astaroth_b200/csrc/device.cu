@@ -33,15 +33,15 @@ acb_host::solve_configs(int* n)
 {
 #if AC_DOUBLE_PRECISION == 1
     static const SolveConfig table[] = {
-        make_solve_config<SolveCfg0, false>("tile32x4_ring8"),
-        make_solve_config<SolveCfg1, false>("tile16x8_ring8"),
-        make_solve_config<SolveCfg2, false>("tile32x2_ring10"),
+        make_solve_config<SolveCfg0, false>(),
+        make_solve_config<SolveCfg1, false>(),
+        make_solve_config<SolveCfg2, false>(),
     };
 #else
     static const SolveConfig table[] = {
-        make_solve_config<SolveCfg0, false>("tile32x8_ring9"),
-        make_solve_config<SolveCfg1, false>("tile32x4_ring10"),
-        make_solve_config<SolveCfg2, false>("tile64x4_ring8"),
+        make_solve_config<SolveCfg0, false>(),
+        make_solve_config<SolveCfg1, false>(),
+        make_solve_config<SolveCfg2, false>(),
     };
 #endif
     *n = (int)(sizeof(table) / sizeof(table[0]));
@@ -68,7 +68,8 @@ struct device_s {
     bool ghost_ok[2];
 
     CUtensorMap tmap[2];
-    int tmap_cfg; // configuration the maps were encoded for (-1: none)
+    CentreMaps cmap[2]; // by parity of `in`: centre boxes over out hi, in lo, out lo
+    int tmap_cfg;       // configuration the maps were encoded for (-1: none)
 
     double* red_partials;
     int red_max_blocks;
@@ -157,6 +158,31 @@ acb_host::encode_block_map(const Layout& L, const state_t* block, const SolveCon
     return AC_SUCCESS;
 }
 
+AcResult
+acb_host::encode_centre_map(const Layout& L, const void* block, const SolveConfig& cfg,
+                            CUtensorMap* map)
+{
+    PFN_encodeTiled_t enc = get_encode_tiled();
+    if (!enc) {
+        fprintf(stderr, "astaroth_b200: cuTensorMapEncodeTiled unavailable\n");
+        return AC_FAILURE;
+    }
+    const cuuint64_t esz     = 4;
+    const cuuint64_t dim[4]  = {(cuuint64_t)L.mxp, (cuuint64_t)L.my, (cuuint64_t)L.mz, ACB_NF};
+    const cuuint64_t str[3]  = {(cuuint64_t)L.mxp * esz, (cuuint64_t)L.plane * esz,
+                               (cuuint64_t)L.fstride * esz};
+    const cuuint32_t box[4]  = {(cuuint32_t)cfg.TX, (cuuint32_t)cfg.TY, 1, ACB_NF};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(block), dim, str,
+                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        fprintf(stderr, "astaroth_b200: cuTensorMapEncodeTiled (centre) failed (%d)\n", (int)r);
+        return AC_FAILURE;
+    }
+    return AC_SUCCESS;
+}
+
 static AcResult
 ensure_maps(const Device d)
 {
@@ -164,9 +190,20 @@ ensure_maps(const Device d)
         return AC_SUCCESS;
     int n;
     const SolveConfig* cfgs = solve_configs(&n);
+    const SolveConfig& cfg = cfgs[d->solve_cfg];
     for (int b = 0; b < 2; ++b)
-        if (encode_block_map(d->L, d->blk[b], cfgs[d->solve_cfg], &d->tmap[b]) != AC_SUCCESS)
+        if (encode_block_map(d->L, d->blk[b], cfg, &d->tmap[b]) != AC_SUCCESS)
             return AC_FAILURE;
+    memset(d->cmap, 0, sizeof(d->cmap));
+    if (cfg.NC > 0) {
+        for (int p = 0; p < 2; ++p) {
+            if (encode_centre_map(d->L, d->blk[p ^ 1], cfg, &d->cmap[p].m[0]) != AC_SUCCESS)
+                return AC_FAILURE;
+            if (d->lo[p] && (encode_centre_map(d->L, d->lo[p], cfg, &d->cmap[p].m[1]) != AC_SUCCESS ||
+                             encode_centre_map(d->L, d->lo[p ^ 1], cfg, &d->cmap[p].m[2]) != AC_SUCCESS))
+                return AC_FAILURE;
+        }
+    }
     d->tmap_cfg = d->solve_cfg;
     return AC_SUCCESS;
 }
@@ -362,7 +399,7 @@ launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e)
     g.nseg  = (g.nzr + g.zseg - 1) / g.zseg;
     g.tasks = ntiles * g.nseg;
     long long grid = std::min(slots, g.tasks);
-    kern<<<(unsigned)grid, cfg.threads, cfg.smem, st>>>(d->tmap[d->cur], a);
+    kern<<<(unsigned)grid, cfg.threads, cfg.smem, st>>>(d->tmap[d->cur], a, d->cmap[d->cur]);
     ACB_CUDA_CHECK(cudaGetLastError());
     d->launches++;
     d->ghost_ok[d->cur ^ 1] = false; // the out block's ghosts are stale now

@@ -32,15 +32,15 @@ acb_host::ensemble_configs(int* n)
 {
 #if AC_DOUBLE_PRECISION == 1
     static const SolveConfig table[] = {
-        make_solve_config<SolveCfg0, true>("tile32x4_ring8"),
-        make_solve_config<SolveCfg1, true>("tile16x8_ring8"),
-        make_solve_config<SolveCfg2, true>("tile32x2_ring10"),
+        make_solve_config<SolveCfg0, true>(),
+        make_solve_config<SolveCfg1, true>(),
+        make_solve_config<SolveCfg2, true>(),
     };
 #else
     static const SolveConfig table[] = {
-        make_solve_config<SolveCfg0, true>("tile32x8_ring9"),
-        make_solve_config<SolveCfg1, true>("tile32x4_ring10"),
-        make_solve_config<SolveCfg2, true>("tile64x4_ring8"),
+        make_solve_config<SolveCfg0, true>(),
+        make_solve_config<SolveCfg1, true>(),
+        make_solve_config<SolveCfg2, true>(),
     };
 #endif
     *n = (int)(sizeof(table) / sizeof(table[0]));
@@ -230,7 +230,10 @@ launch_solve_all(Ensemble e, cudaStream_t st, int step, AcReal dt)
     a.nmembers            = (int)e->m.size();
     a.total_tasks         = e->total_tasks;
     // the map parameter is not read in ensemble mode; any valid map fills it
-    cfg.kern[step]<<<e->grid, cfg.threads, cfg.smem, st>>>(e->h_desc[e->cur][0].tmap, a);
+    // ensemble kernels take their centre values by plain loads: no centre maps
+    static const CentreMaps no_centre_maps = {};
+    cfg.kern[step]<<<e->grid, cfg.threads, cfg.smem, st>>>(e->h_desc[e->cur][0].tmap, a,
+                                                            no_centre_maps);
     ACB_CUDA_CHECK(cudaGetLastError());
     e->launches++;
     e->ghost_ok[e->cur ^ 1] = false; // the out blocks' ghosts are stale now

@@ -3,6 +3,7 @@
 // encoding, kernel arguments from a parameter mirror, the work split, and the
 // flat <-> padded copies.
 #pragma once
+#include <stdio.h>
 #include "astaroth.h"
 #include "common.cuh"
 #include "solve.cuh"
@@ -12,34 +13,53 @@
 using SolveCfg0 = TileCfg<32, 4, 8, 1>;
 using SolveCfg1 = TileCfg<16, 8, 8, 1>;
 using SolveCfg2 = TileCfg<32, 2, 10, 2>;
+#elif ACB_MIXED
+// the first and last stage the centre values of substeps 1 and 2 by TMA
+using SolveCfg0 = TileCfg<32, 8, 7, 1, 3>;
+using SolveCfg1 = TileCfg<32, 8, 9, 1>;
+using SolveCfg2 = TileCfg<64, 4, 6, 1, 3>;
 #else
 using SolveCfg0 = TileCfg<32, 8, 9, 1>;
-using SolveCfg1 = TileCfg<32, 4, 10, 1>;
-using SolveCfg2 = TileCfg<64, 4, 8, 1>;
+using SolveCfg1 = TileCfg<64, 4, 8, 1>;
+using SolveCfg2 = TileCfg<32, 8, 7, 1>;
 #endif
 
-typedef void (*SolveKernelFn)(const CUtensorMap, const SolveArgs<AcReal>);
+typedef void (*SolveKernelFn)(const CUtensorMap, const SolveArgs<AcReal>, const CentreMaps);
 
 struct SolveConfig {
     const char* name;
     int TX, TY, NP, threads;
     int launch_regs; // registers a thread the kernels must be launched with (0: any)
+    int NC;          // centre ring slots (0: the centre values are plain loads)
     size_t smem;
     SolveKernelFn kern[4]; // substeps 0, 1, 2, and 2 with helical forcing (single mesh only)
 };
 
+// "tile32x8_ring9", "..._tmacentre" when the centre values are staged by TMA
+template <class Cfg, bool ENS>
+const char*
+solve_config_name()
+{
+    static char buf[48];
+    if (!buf[0])
+        snprintf(buf, sizeof(buf), "tile%dx%d_ring%d%s", Cfg::TX, Cfg::TY, Cfg::NP,
+                 (!ENS && Cfg::NC > 0) ? "_tmacentre" : "");
+    return buf;
+}
+
 template <class Cfg, bool ENS>
 SolveConfig
-make_solve_config(const char* name)
+make_solve_config()
 {
     SolveConfig c;
-    c.name    = name;
+    c.name    = solve_config_name<Cfg, ENS>();
     c.TX      = Cfg::TX;
     c.TY      = Cfg::TY;
     c.NP      = Cfg::NP;
     c.threads = Cfg::THREADS;
     c.launch_regs = Cfg::REG_LAUNCH;
-    c.smem    = Cfg::smem_bytes();
+    c.NC          = ENS ? 0 : Cfg::NC;
+    c.smem    = ENS ? Cfg::ring_bytes() : Cfg::smem_bytes(); // ensembles load centres directly
     c.kern[0] = solve_kernel<Cfg, 0, ENS>;
     c.kern[1] = solve_kernel<Cfg, 1, ENS>;
     c.kern[2] = solve_kernel<Cfg, 2, ENS>;
@@ -64,6 +84,9 @@ AcResult prepare_table(const SolveConfig* cfgs, int n);
 // 4-D map (x, y, z, field) over a field block with a (TX+8, TY+6, 1, 8) box
 AcResult encode_block_map(const Layout& L, const state_t* block, const SolveConfig& cfg,
                           CUtensorMap* map);
+// the same with a (TX, TY, 1, 8) box: a tile's centre values (4-byte elements)
+AcResult encode_centre_map(const Layout& L, const void* block, const SolveConfig& cfg,
+                           CUtensorMap* map);
 
 // kernel arguments from a parameter mirror: coefficients pre-scaled in double
 // and rounded once to AcReal; rkA/rkB for `step` from AC_dt

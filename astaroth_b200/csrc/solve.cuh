@@ -93,9 +93,34 @@ struct SolveArgs {
     long long total_tasks;
 };
 
-template <int TX_, int TY_, int NP_, int MINB_>
+// Centre-only arrays of a substep that the ring does not carry: the previous
+// state (s > 0) and, in the mixed build, the lo parts of `in` and (s > 0) of
+// `out`. Map slots: 0 = out hi, 1 = in lo, 2 = out lo.
+template <int STEP>
+struct CentreSet {
+    static constexpr bool PREV = STEP > 0;
+    static constexpr bool LO   = ACB_MIXED != 0;
+    static constexpr int N     = (PREV ? 1 : 0) + (LO ? (PREV ? 2 : 1) : 0);
+    // staged by TMA only where it pays (measured at 512^3): the three arrays of
+    // mixed substeps 1 and 2; one array is cheaper as plain loads
+    static constexpr bool STAGE = N == 3;
+    // position of each map's array in a centre slot (-1: not loaded)
+    static constexpr int POS_PREV    = PREV ? 0 : -1;
+    static constexpr int POS_CUR_LO  = LO ? (PREV ? 1 : 0) : -1;
+    static constexpr int POS_PREV_LO = (LO && PREV) ? 2 : -1;
+};
+
+struct CentreMaps {
+    CUtensorMap m[3]; // (TX, TY, 1, 8) boxes over out hi, in lo, out lo
+};
+
+template <int TX_, int TY_, int NP_, int MINB_, int NC_ = 0>
 struct TileCfg {
     static constexpr int TX = TX_, TY = TY_, NP = NP_, MINB = MINB_;
+    // NC > 0: the centre-only values of single-mesh single-precision substeps
+    // arrive by TMA in a ring of NC output-plane slots (else plain loads)
+    static constexpr int NC = NC_;
+    static constexpr int CENTRE = TX_ * TY_ * ACB_NF; // elements of one centre array
     static constexpr int BX = TX_ + 8, BY = TY_ + 6;
     static constexpr int CONSUMERS = TX_ * TY_;        // one thread per (x, y) column
     static constexpr int CWARPS    = CONSUMERS / 32;   // consumer warps
@@ -112,7 +137,12 @@ struct TileCfg {
         WGSPEC ? (REG_CONSUMER * CONSUMERS + REG_PRODUCER * 128 + THREADS - 1) / THREADS : 0;
     static constexpr int FIELD   = BX * BY;
     static constexpr int PLANE   = ACB_NF * FIELD; // elements per ring slot
-    static constexpr size_t smem_bytes() { return (size_t)NP * PLANE * sizeof(state_t); }
+    static constexpr size_t ring_bytes() { return (size_t)NP * PLANE * sizeof(state_t); }
+    static constexpr size_t centre_slot_bytes()
+    {
+        return (size_t)(ACB_MIXED ? 3 : 1) * CENTRE * sizeof(float);
+    }
+    static constexpr size_t smem_bytes() { return ring_bytes() + NC * centre_slot_bytes(); }
 };
 
 namespace acb {
@@ -651,8 +681,11 @@ template <class Cfg, int STEP, bool ENS>
 __device__ __forceinline__ bool
 consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<AcReal>& P,
              long long lt, state_t* out, float* in_lo, float* out_lo, const state_t* ring,
-             uint64_t* full, uint64_t* empty, volatile int* abort_flag, uint32_t& q)
+             uint64_t* full, uint64_t* empty, volatile int* abort_flag, uint32_t& q,
+             const float* centre, uint64_t* full_c, uint64_t* empty_c, uint32_t& oq)
 {
+    using CS          = CentreSet<STEP>;
+    constexpr bool CT = Cfg::NC > 0 && !ENS && CS::STAGE;
     using T = AcReal;
     constexpr int TX = Cfg::TX, NP = Cfg::NP, BX = Cfg::BX;
     constexpr int FIELD = Cfg::FIELD, PLANE = Cfg::PLANE;
@@ -708,6 +741,12 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
             ok = mbar_wait_bounded(&full[l % NP], (l / NP) & 1u);
             ok = __all_sync(0xffffffffu, ok);
         }
+        if constexpr (CT) {
+            if (ok) {
+                ok = mbar_wait_bounded(&full_c[oq % Cfg::NC], (oq / Cfg::NC) & 1u);
+                ok = __all_sync(0xffffffffu, ok);
+            }
+        }
         if (!ok || *abort_flag) {
             if (lane == 0) {
                 atomicOr(a.status, (unsigned)ACB_STATUS_TMA_TIMEOUT);
@@ -725,6 +764,24 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
                 cv = cv_next;
                 if (p + 1 < tg.nout)
                     load_centre<STEP>(L, out, in_lo, out_lo, id + L.plane, cv_next);
+            }
+            else if constexpr (CT) {
+                // from the centre slot the producer filled by TMA
+                const float* cs = centre + (size_t)(oq % Cfg::NC) * (Cfg::centre_slot_bytes() / 4) +
+                                  ty * TX + tx;
+                constexpr int FS = Cfg::TX * Cfg::TY;
+#pragma unroll
+                for (int f = 0; f < ACB_NF; ++f) {
+                    if constexpr (CS::PREV)
+                        cv.prev[f] = cs[CS::POS_PREV * Cfg::CENTRE + f * FS];
+#if ACB_MIXED
+                    cv.cur_lo[f] = cs[CS::POS_CUR_LO * Cfg::CENTRE + f * FS];
+                    if constexpr (CS::PREV)
+                        cv.prev_lo[f] = cs[CS::POS_PREV_LO * Cfg::CENTRE + f * FS];
+                    else
+                        cv.prev_lo[f] = 0.f;
+#endif
+                }
             }
             else {
                 load_centre<STEP>(L, out, in_lo, out_lo, id, cv);
@@ -779,6 +836,11 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
         // plane three below it
         if (lane == 0)
             mbar_arrive(&empty[(q + p + (QZ ? NGHOST : 0)) % NP]);
+        if constexpr (CT) {
+            if (lane == 0)
+                mbar_arrive(&empty_c[oq % Cfg::NC]);
+            ++oq;
+        }
     }
     // the planes of the task not released yet
     __syncwarp();
@@ -801,7 +863,8 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
 // map, geometry, buffers and parameters from the descriptor table.
 template <class Cfg, int STEP, bool ENS>
 __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
-    solve_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ SolveArgs<AcReal> a)
+    solve_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ SolveArgs<AcReal> a,
+                 const __grid_constant__ CentreMaps cm)
 {
     using T = AcReal;
     constexpr int TX = Cfg::TX, NP = Cfg::NP, BX = Cfg::BX;
@@ -812,6 +875,14 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     state_t* ring = reinterpret_cast<state_t*>(smem_raw);
     __shared__ __align__(8) uint64_t full[NP];
     __shared__ __align__(8) uint64_t empty[NP];
+    // centre ring (CT): one slot per output plane, filled by the producer
+    // together with the deepest stencil plane that output needs
+    using CS             = CentreSet<STEP>;
+    constexpr bool CT    = Cfg::NC > 0 && !ENS && CS::STAGE;
+    constexpr int NCS    = CT ? Cfg::NC : 1;
+    __shared__ __align__(8) uint64_t full_c[NCS];
+    __shared__ __align__(8) uint64_t empty_c[NCS];
+    float* centre = reinterpret_cast<float*>(smem_raw + Cfg::ring_bytes());
     __shared__ volatile int abort_flag;
     __shared__ SolveParams<T> sP[CWARPS]; // ensemble: each consumer warp's copy of its member's parameters
 
@@ -822,6 +893,10 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
         for (int s = 0; s < NP; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], CWARPS);
+        }
+        for (int s = 0; s < NCS; ++s) {
+            mbar_init(&full_c[s], 1);
+            mbar_init(&empty_c[s], CWARPS);
         }
         fence_barrier_init();
         abort_flag = 0;
@@ -844,6 +919,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
             if (!ENS)
                 prefetch_tensormap(&tin);
             uint32_t q  = 0;
+            uint32_t oq = 0; // output planes whose centre arrays were issued
             bool ok     = true;
             int last_m  = -1;
             for (long long t = blockIdx.x; t < ntasks && ok; t += gridDim.x) {
@@ -880,6 +956,32 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
                     tma_load_4d(ring + (size_t)s * PLANE, map, xt, yt, tg.k0 - NGHOST + l, 0,
                                 &full[s]);
                     ++q;
+                    if constexpr (CT) {
+                        // plane l is the top one output l - 6 needs: its centre
+                        // arrays go out now, into the next centre slot
+                        if (l >= 2 * NGHOST) {
+                            const uint32_t sc = oq % Cfg::NC, usec = oq / Cfg::NC;
+                            if (usec > 0 && !mbar_wait_bounded(&empty_c[sc], (usec - 1) & 1u)) {
+                                ok = false;
+                                break;
+                            }
+                            constexpr uint32_t CB = Cfg::CENTRE * sizeof(float);
+                            float* dst   = centre + (size_t)sc * (Cfg::centre_slot_bytes() / 4);
+                            const int xc = g->L.offx + tg.i0; // interior tile start: 32-byte aligned
+                            const int zc = tg.k0 + (l - 2 * NGHOST);
+                            mbar_arrive_expect_tx(&full_c[sc], CS::N * CB);
+                            if (CS::PREV)
+                                tma_load_4d(dst + CS::POS_PREV * Cfg::CENTRE, &cm.m[0], xc, tg.j0,
+                                            zc, 0, &full_c[sc]);
+                            if (CS::LO)
+                                tma_load_4d(dst + CS::POS_CUR_LO * Cfg::CENTRE, &cm.m[1], xc,
+                                            tg.j0, zc, 0, &full_c[sc]);
+                            if (CS::LO && CS::PREV)
+                                tma_load_4d(dst + CS::POS_PREV_LO * Cfg::CENTRE, &cm.m[2], xc,
+                                            tg.j0, zc, 0, &full_c[sc]);
+                            ++oq;
+                        }
+                    }
                 }
             }
             if (!ok) {
@@ -888,13 +990,16 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
                 // wait (bounded) for this CTA's loads still in flight before leaving
                 for (uint32_t r = q > (uint32_t)NP ? q - NP : 0; r < q; ++r)
                     (void)mbar_wait_bounded(&full[r % NP], (r / NP) & 1u);
+                if constexpr (CT)
+                    for (uint32_t r = oq > (uint32_t)Cfg::NC ? oq - Cfg::NC : 0; r < oq; ++r)
+                        (void)mbar_wait_bounded(&full_c[r % Cfg::NC], (r / Cfg::NC) & 1u);
             }
         }
         return;
     }
 
     // ---------------------------------------------------------------- consumers
-    uint32_t q = 0;
+    uint32_t q = 0, oq = 0;
     for (long long t = blockIdx.x; t < ntasks; t += gridDim.x) {
         bool ok;
         if constexpr (ENS) {
@@ -910,11 +1015,12 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
             const SolveGeom gv = md->g;
             ok = consume_task<Cfg, STEP, ENS>(a, gv, sP[warp], t - md->task_begin, md->out,
                                               md->in_lo, md->out_lo, ring, full, empty,
-                                              &abort_flag, q);
+                                              &abort_flag, q, centre, full_c, empty_c, oq);
         }
         else {
             ok = consume_task<Cfg, STEP, ENS>(a, a.g, a.P, t, a.out, a.in_lo, a.out_lo, ring, full,
-                                              empty, &abort_flag, q);
+                                              empty, &abort_flag, q, centre, full_c, empty_c,
+                                              oq);
         }
         if (!ok)
             return;
