@@ -136,6 +136,34 @@ halo_unit(const Layout& L, state_t* block, float* lo, unsigned units_a, unsigned
         const int k          = NGHOST + (int)kq;
         const long long base = lidx(L, 0, j, k) + (long long)f * L.fstride;
         state_t* F           = block + base;
+        if constexpr (sizeof(state_t) == 4) {
+            if ((L.nx & 3) == 0) {
+                // 4-byte elements (offx = 5), nx % 4 == 0: x = -1..2 and
+                // x = nx+3..nx+6 are aligned 16-byte groups of the row (x = -1
+                // and x = nx+6 are row padding, inside the row, and get their
+                // periodic images too); their sources x = nx-1..nx+2 and
+                // x = 3..6 are aligned groups as well. Group of x: (offx + x) / 4.
+                const int gl    = (L.offx - 1) >> 2;        // x = -1
+                const int gr    = (L.offx + L.nx + 3) >> 2; // x = nx + 3
+                const int sl    = (L.offx + L.nx - 1) >> 2; // x = nx - 1
+                const int sr    = (L.offx + 3) >> 2;        // x = 3
+                float4* R       = reinterpret_cast<float4*>(F - L.offx);
+                const float4 vl = R[sl];
+                const float4 vr = R[sr];
+#if ACB_MIXED
+                float4* G       = reinterpret_cast<float4*>(lo + base - L.offx);
+                const float4 wl = G[sl];
+                const float4 wr = G[sr];
+#endif
+                R[gl] = vl;
+                R[gr] = vr;
+#if ACB_MIXED
+                G[gl] = wl;
+                G[gr] = wr;
+#endif
+                return;
+            }
+        }
         state_t v[2 * NGHOST];
 #pragma unroll
         for (int q = 0; q < NGHOST; ++q) {

@@ -489,7 +489,9 @@ def run_ours(args) -> None:
     alg = alg_bytes_per_step("mixed", n)
     achieved_gbs = alg * args.steps / (res["solve_ms_total"] * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    traffic = profile_traffic("solve_mixed_512.md")
+    # DRAM bytes of one s = 1 launch at this size, from the committed ncu
+    # summary of a 256^3 capture scaled by the cells (bytes grow with them)
+    traffic = profile_traffic("solve_mixed_256.md")
 
     variants = {}
     errors = None
