@@ -109,6 +109,25 @@ def mesh_type(prec: Precision):
     return AcMeshD if prec.double else AcMeshF
 
 
+def _forcing_fields(R):
+    return [("magnitude", R), ("k_force", R * 3), ("ff_hel_re", R * 3), ("ff_hel_im", R * 3),
+            ("phase", R), ("kaver", R)]
+
+
+class AcForcingParamsF(C.Structure):
+    """include/astaroth_b200.h AcForcingParams, single-precision builds."""
+    _fields_ = _forcing_fields(C.c_float)
+
+
+class AcForcingParamsD(C.Structure):
+    """include/astaroth_b200.h AcForcingParams, double-precision build."""
+    _fields_ = _forcing_fields(C.c_double)
+
+
+def forcing_type(prec: Precision):
+    return AcForcingParamsD if prec.double else AcForcingParamsF
+
+
 def real3_type(prec: Precision):
     return _D_REAL3 if prec.double else _F_REAL3
 

@@ -33,7 +33,7 @@ FLAVOURS = {
     "mixed": ["-DAC_DOUBLE_PRECISION=0", "-DACB_MIXED=1"],
 }
 CU_SOURCES = ["device.cu", "ensemble.cu", "reduce_noalloc.cu"]
-CXX_SOURCES = ["node.cc", "host_utils.cc", "host_model.cc"]
+CXX_SOURCES = ["node.cc", "host_utils.cc", "host_model.cc", "forcing.cc"]
 HEADERS = ["common.cuh", "tma.cuh", "solve.cuh", "halo.cuh", "reduce.cuh", "internal.cuh"]
 
 NVCC_FLAGS = [

@@ -1327,6 +1327,27 @@ acDeviceSetForcing(const Device device, const int enabled)
     return AC_SUCCESS;
 }
 
+AcResult
+acDeviceLoadForcingParams(const Device device, const Stream stream, const AcForcingParams params)
+{
+    const struct {
+        AcRealParam param;
+        AcReal value;
+    } v[] = {
+        {AC_forcing_magnitude, params.magnitude}, {AC_forcing_phase, params.phase},
+        {AC_k_forcex, params.k_force[0]},         {AC_k_forcey, params.k_force[1]},
+        {AC_k_forcez, params.k_force[2]},         {AC_ff_hel_rex, params.ff_hel_re[0]},
+        {AC_ff_hel_rey, params.ff_hel_re[1]},     {AC_ff_hel_rez, params.ff_hel_re[2]},
+        {AC_ff_hel_imx, params.ff_hel_im[0]},     {AC_ff_hel_imy, params.ff_hel_im[1]},
+        {AC_ff_hel_imz, params.ff_hel_im[2]},     {AC_kaver, params.kaver},
+    };
+    AcResult rc = AC_SUCCESS;
+    for (const auto& e : v)
+        if (acDeviceLoadScalarUniform(device, stream, e.param, e.value) != AC_SUCCESS)
+            rc = AC_FAILURE;
+    return rc;
+}
+
 static AcResult
 enqueue_step(const Device d, cudaStream_t st)
 {

@@ -55,6 +55,7 @@ ASTAROTH_B200_H = [
     "acDeviceGetMemoryFootprint", "acDeviceIntegrateStep", "acDeviceIntegrateSteps",
     "acDeviceSetForcing", "acDeviceLoadVertexBufferDouble", "acDeviceStoreVertexBufferDouble",
     "acDeviceReduceScalDouble", "acDeviceReduceVecDouble", "acReduceScalNoAlloc",
+    "acForcingParamsFromUniforms", "acForcingParamsGenerate", "acDeviceLoadForcingParams",
     "acEnsembleCreate", "acEnsembleDestroy", "acEnsembleLoadMember", "acEnsembleStoreMember",
     "acEnsembleIntegrateStep", "acEnsembleIntegrateSteps", "acEnsembleSynchronize",
     "acEnsembleGetStatus", "acEnsembleGetCudaStream", "acEnsembleGetLaunchCount",
@@ -71,6 +72,7 @@ def _declare(lib: C.CDLL, prec: abi.Precision) -> None:
     R = prec.real
     Info = abi.info_type(prec)
     Mesh = abi.mesh_type(prec)
+    Frc = abi.forcing_type(prec)
     I3 = abi.int3
     Dev = C.c_void_p
     res = C.c_int
@@ -160,6 +162,9 @@ def _declare(lib: C.CDLL, prec: abi.Precision) -> None:
         "acDeviceReduceScalDouble": (res, [Dev, i, i, i, C.POINTER(C.c_double)]),
         "acDeviceReduceVecDouble": (res, [Dev, i, i, i, i, i, C.POINTER(C.c_double)]),
         "acReduceScalNoAlloc": (res, [C.c_void_p, i, C.c_void_p, i, i, i, C.c_void_p]),
+        "acForcingParamsFromUniforms": (res, [Info, C.POINTER(R), C.POINTER(Frc)]),
+        "acForcingParamsGenerate": (res, [Info, C.POINTER(C.c_ulonglong), C.POINTER(Frc)]),
+        "acDeviceLoadForcingParams": (res, [Dev, i, Frc]),
         # ensembles
         "acEnsembleCreate": (res, [i, i, C.POINTER(Info), C.POINTER(Dev)]),
         "acEnsembleDestroy": (res, [Dev]),

@@ -56,6 +56,39 @@ AcResult acDeviceIntegrateSteps(const Device device, const Stream stream, const 
  * AC_ff_hel_* / AC_kaver uniforms. */
 AcResult acDeviceSetForcing(const Device device, const int enabled);
 
+/* Helical forcing parameters of one step: replaces the reference standalone's
+ * ForcingParams / generateForcingParams / loadForcingParamsToDevice
+ * (samples/standalone/model/host_forcing.h:57-64, host_forcing.cc:287-320,
+ * :215-235). */
+typedef struct {
+    AcReal magnitude;
+    AcReal k_force[3];
+    AcReal ff_hel_re[3];
+    AcReal ff_hel_im[3];
+    AcReal phase;
+    AcReal kaver;
+} AcForcingParams;
+
+/* generateForcingParams with its five random draws given: u[0..2] the
+ * wavevector's azimuth, polar angle and length, u[3] the phase, u[4] the angle
+ * of e about k, each in [0, 1] (the reference draws them in this order from
+ * rand() / RAND_MAX). Reads AC_relhel, AC_forcing_magnitude, AC_kmin, AC_kmax
+ * from `info`. */
+AcResult acForcingParamsFromUniforms(const AcMeshInfo info, const AcReal u[5],
+                                     AcForcingParams* params);
+
+/* The same with the draws from a seeded counter-based generator: *state is
+ * the seed on the first call and advances by five draws per call, so a run is
+ * reproducible from its seed (the reference's rand() stream is not). */
+AcResult acForcingParamsGenerate(const AcMeshInfo info, unsigned long long* state,
+                                 AcForcingParams* params);
+
+/* loadForcingParamsToDevice for one Device: loads the AC_forcing_magnitude,
+ * AC_forcing_phase, AC_k_force*, AC_ff_hel_* and AC_kaver uniforms. Forcing
+ * is applied only while acDeviceSetForcing(device, 1) is in effect. */
+AcResult acDeviceLoadForcingParams(const Device device, const Stream stream,
+                                   const AcForcingParams params);
+
 /* ---- ensembles ------------------------------------------------------------
  * Many independent meshes (members) of possibly different sizes and
  * parameters on one GPU, advanced together: each substep is ONE ghost-fill
