@@ -524,15 +524,18 @@ acb_host::copy_field_range(cudaStream_t st, const Layout& L, state_t* field, siz
     const size_t w   = sizeof(state_t);
     const size_t dpw = (size_t)L.mxp * w, hpw = (size_t)L.mx * w;
     return for_each_row_run(L, s, count, [&](size_t dev, size_t t, size_t n, size_t rows) {
+        // cudaMemcpyDefault: the caller's mesh buffers are normally host
+        // memory, but a device-resident mesh (unified addressing) is copied
+        // device to device the same way
         cudaError_t err;
         if (rows == 1)
-            err = h2d ? cudaMemcpyAsync(field + dev, host + t, n * w, cudaMemcpyHostToDevice, st)
-                      : cudaMemcpyAsync(host + t, field + dev, n * w, cudaMemcpyDeviceToHost, st);
+            err = h2d ? cudaMemcpyAsync(field + dev, host + t, n * w, cudaMemcpyDefault, st)
+                      : cudaMemcpyAsync(host + t, field + dev, n * w, cudaMemcpyDefault, st);
         else
             err = h2d ? cudaMemcpy2DAsync(field + dev, dpw, host + t, hpw, n * w, rows,
-                                          cudaMemcpyHostToDevice, st)
+                                          cudaMemcpyDefault, st)
                       : cudaMemcpy2DAsync(host + t, hpw, field + dev, dpw, n * w, rows,
-                                          cudaMemcpyDeviceToHost, st);
+                                          cudaMemcpyDefault, st);
         if (err == cudaSuccess && h2d && lo_field) // fresh values carry no lo part
             err = cudaMemset2DAsync(lo_field + dev, (size_t)L.mxp * sizeof(float), 0,
                                     n * sizeof(float), rows, st);

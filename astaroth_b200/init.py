@@ -83,28 +83,33 @@ def workload_fields_torch(nx: int, ny: int, nz: int, dtype, seed: int = 1,
                           amplitude: float = 1e-3, velocity_mode: float = 0.0, device="cuda"):
     """Torch twin of workload_fields: returns eight (nz+6, ny+6, nx+6) tensors of
     `dtype` (a torch dtype) with periodic ghosts, equal to the numpy version."""
+    return [workload_field_torch(w, nx, ny, nz, dtype, seed, amplitude, velocity_mode, device)
+            for w in range(NUM_VTXBUF_HANDLES)]
+
+
+def workload_field_torch(w: int, nx: int, ny: int, nz: int, dtype, seed: int = 1,
+                         amplitude: float = 1e-3, velocity_mode: float = 0.0, device="cuda"):
+    """Field w of workload_fields_torch alone (for meshes too large to hold
+    all eight initial fields beside the solver's state)."""
     import torch
 
-    out = []
-    for w in range(NUM_VTXBUF_HANDLES):
-        f = noise_interior_torch(seed, w, nx, ny, nz, amplitude, device)
-        if velocity_mode and w in (1, 2, 3):
-            axis, n = {1: ("y", ny), 2: ("z", nz), 3: ("x", nx)}[w]
-            s = velocity_mode * torch.sin(
-                2.0 * (2.0 * math.pi / n) * torch.arange(n, dtype=torch.float64, device=device))
-            if axis == "x":
-                f += s[None, None, :]
-            elif axis == "y":
-                f += s[None, :, None]
-            else:
-                f += s[:, None, None]
-        g = f.to(dtype)
-        del f
-        g = torch.cat([g[-NGHOST:], g, g[:NGHOST]], dim=0)
-        g = torch.cat([g[:, -NGHOST:], g, g[:, :NGHOST]], dim=1)
-        g = torch.cat([g[:, :, -NGHOST:], g, g[:, :, :NGHOST]], dim=2)
-        out.append(g.contiguous())
-    return out
+    f = noise_interior_torch(seed, w, nx, ny, nz, amplitude, device)
+    if velocity_mode and w in (1, 2, 3):
+        axis, n = {1: ("y", ny), 2: ("z", nz), 3: ("x", nx)}[w]
+        s = velocity_mode * torch.sin(
+            2.0 * (2.0 * math.pi / n) * torch.arange(n, dtype=torch.float64, device=device))
+        if axis == "x":
+            f += s[None, None, :]
+        elif axis == "y":
+            f += s[None, :, None]
+        else:
+            f += s[:, None, None]
+    g = f.to(dtype)
+    del f
+    g = torch.cat([g[-NGHOST:], g, g[:NGHOST]], dim=0)
+    g = torch.cat([g[:, -NGHOST:], g, g[:, :NGHOST]], dim=1)
+    g = torch.cat([g[:, :, -NGHOST:], g, g[:, :, :NGHOST]], dim=2)
+    return g.contiguous()
 
 
 def wrap_ghosts(interior: np.ndarray) -> np.ndarray:

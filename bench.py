@@ -11,11 +11,13 @@ FP32 libraries run the same steps beside it for the comparison and the error.
 
 One step = three substeps, each a periodic ghost fill of all fields plus one
 fused solve launch, all through the C ABI (acDevicePeriodicBoundconds,
-acDeviceIntegrateSubstep, acDeviceSwapBuffers). A substep over the whole
-interior also stores its results to their periodic ghost images, so after the
-first substep the ghost-fill call finds the ghosts valid and launches nothing.
-Inputs are larger than L2 (8.9 GB of state per block), so no L2 flush is
-needed between steps.
+acDeviceIntegrateSubstep, acDeviceSwapBuffers). Inputs are larger than L2
+(8.9 GB of state per block), so no L2 flush is needed between steps.
+
+Beside the headline line: the FP64 and FP32 libraries on the same steps (and
+the per-field error against FP64), an end-to-end run from pinned host memory,
+the 64-member ensemble, and the forced large-mesh run (1024^3 mixed, helical
+forcing from a seeded generator and four FP64 diagnostics every step).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -56,6 +58,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-member ensemble")
+    ap.add_argument("--no-forced", action="store_true",
+                    help="skip the forced large-mesh run (helical forcing + diagnostics)")
+    ap.add_argument("--forced-n", type=int, default=1024, help="mesh size of the forced run")
     return ap.parse_args(argv)
 
 
@@ -417,6 +422,89 @@ def ensemble_run(steps: int, ranks) -> dict:
             "speedup_vs_loop_sync": loop_sync / ens_ms}
 
 
+def forced_run(n: int, steps: int, warmup: int, ranks, gpu: int) -> dict:
+    """The forced large-mesh workload: an n^3 mixed-precision mesh (1024^3:
+    141 GB of (hi, lo) state in two buffers), the seeded initial state of the
+    headline workload, and every step a new helical forcing (|k| in [1, 3],
+    magnitude 0.05, relhel 0, from the seeded generator acForcingParamsGenerate,
+    seed 5) then one RK3 step then the diagnostics: max, min and rms of |u|
+    and rms_exp of lnrho (FP64 reductions, each read back). The initial fields
+    are generated on the device one at a time and loaded device to device."""
+    import ctypes as C
+
+    import torch
+
+    from astaroth_b200 import Device, abi, init
+    from astaroth_b200.device import ForcingGenerator
+
+    prec = abi.PRECISIONS["mixed"]
+    ds = 2.0 * math.pi / n
+    info = abi.make_info(prec, n, n, n, dsx=ds, dsy=ds, dsz=ds, kmin=1.0, kmax=3.0, relhel=0.0,
+                         forcing_magnitude=0.05, **PHYS)
+    torch.cuda.empty_cache()
+    free_b, _ = torch.cuda.mem_get_info(gpu)
+    dev = Device("mixed", info, gpu)
+    try:
+        footprint = dev.memory_footprint()
+        mesh = abi.mesh_type(prec)()
+        mesh.info = info
+        for w in range(abi.NUM_VTXBUF_HANDLES):
+            g = init.workload_field_torch(w, n, n, n, torch.float32, seed=1, amplitude=1e-3,
+                                          velocity_mode=0.1, device=f"cuda:{gpu}")
+            torch.cuda.synchronize(gpu)
+            mesh.vertex_buffer[w] = C.cast(C.c_void_p(g.data_ptr()), C.POINTER(prec.real))
+            if dev.lib.acDeviceLoadVertexBuffer(dev.handle, 0, mesh, w) != abi.AC_SUCCESS:
+                raise RuntimeError("acDeviceLoadVertexBuffer failed")
+            dev.synchronize()
+            mesh.vertex_buffer[w] = C.POINTER(prec.real)()
+            del g
+            torch.cuda.empty_cache()
+        dev.set_forcing(True)
+        gen = ForcingGenerator("mixed", info, seed=5)
+        st = torch.cuda.ExternalStream(dev.cuda_stream(0))
+        diag = {}
+
+        def step():
+            dev.load_forcing_params(gen.next())
+            dev.integrate_step(DT)
+            diag["umax"] = dev.reduce_vec_double(abi.RTYPE_MAX, abi.VTXBUF_UUX, abi.VTXBUF_UUY,
+                                                 abi.VTXBUF_UUZ)
+            diag["umin"] = dev.reduce_vec_double(abi.RTYPE_MIN, abi.VTXBUF_UUX, abi.VTXBUF_UUY,
+                                                 abi.VTXBUF_UUZ)
+            diag["urms_sum"] = dev.reduce_vec_double(abi.RTYPE_RMS, abi.VTXBUF_UUX,
+                                                     abi.VTXBUF_UUY, abi.VTXBUF_UUZ)
+            diag["rhorms_sum"] = dev.reduce_scal_double(abi.RTYPE_RMS_EXP, abi.VTXBUF_LNRHO)
+
+        for _ in range(warmup):
+            step()
+        dev.synchronize()
+        ranks.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(st)
+        for _ in range(steps):
+            step()
+        e1.record(st)
+        e1.synchronize()
+        wall_ms = (time.perf_counter() - t0) * 1e3
+        ranks.barrier()
+        ms = ranks.max(e0.elapsed_time(e1))
+        cells = n ** 3
+        return {"mesh": [n, n, n], "steps": steps, "warmup": warmup,
+                "ms_per_step": ms / steps, "wall_ms_per_step": wall_ms / steps,
+                "cell_updates_per_s": ranks.world * cells * steps / (ms * 1e-3),
+                "device_state_gb": footprint / 1e9, "free_gb_before": free_b / 1e9,
+                "step": "forcing params load + 3 x (ghost fill + forced solve) + 4 FP64 "
+                        "reductions read back",
+                "forcing": "helical, |k| in [1, 3], magnitude 0.05, relhel 0, seed 5",
+                "last_step_diagnostics": {"umax": diag["umax"], "umin": diag["umin"],
+                                          "urms": math.sqrt(diag["urms_sum"] / cells),
+                                          "rho_rms": math.sqrt(diag["rhorms_sum"] / cells)}}
+    finally:
+        dev.destroy()
+        torch.cuda.empty_cache()
+
+
 def profile_traffic(name: str):
     """Per-launch DRAM bytes of the dominant kernel from a committed ncu
     summary (a line `traffic_bytes_per_launch: <value>`), else None."""
@@ -538,6 +626,11 @@ def run_ours(args) -> None:
     if not args.no_ensemble:
         ensemble = ensemble_run(min(args.steps, 20), ranks)
 
+    forced = None
+    if not args.no_forced:
+        torch.cuda.empty_cache()
+        forced = forced_run(args.forced_n, min(args.steps, 20), max(args.warmup, 3), ranks, gpu)
+
     cpu = None
     if ranks.rank == 0 and not args.no_cpu:
         c = cpu_reference_sample(budget_s=12.0)
@@ -557,7 +650,7 @@ def run_ours(args) -> None:
                              "solve_ms_per_substep": res["solve_ms_per_substep"]},
                 "clocks": res["clocks"], "gpu_launches": res["launches"],
                 "e2e": e2e, "cpu_baseline": cpu, "variants": variants, "errors": errors,
-                "ensemble": ensemble}
+                "ensemble": ensemble, "forced": forced}
         print(json.dumps(line), flush=True)
     ranks.close()
 
