@@ -132,32 +132,6 @@ class Device:
                "acDeviceLoadForcingParams")
 
 
-def forcing_params_from_uniforms(flavour: str, info, u) -> object:
-    """acForcingParamsFromUniforms: the step's forcing from five draws in [0, 1]."""
-    prec = abi.PRECISIONS[flavour]
-    lib = library.load(flavour)
-    out = abi.forcing_type(prec)()
-    arr = (prec.real * 5)(*[float(x) for x in u])
-    _check(lib.acForcingParamsFromUniforms(info, arr, C.byref(out)), "acForcingParamsFromUniforms")
-    return out
-
-
-class ForcingGenerator:
-    """acForcingParamsGenerate: a reproducible stream of per-step forcing
-    parameters from a seed."""
-
-    def __init__(self, flavour: str, info, seed: int):
-        self.prec = abi.PRECISIONS[flavour]
-        self.lib = library.load(flavour)
-        self.info = info
-        self.state = C.c_ulonglong(seed)
-
-    def next(self):
-        out = abi.forcing_type(self.prec)()
-        _check(self.lib.acForcingParamsGenerate(self.info, C.byref(self.state), C.byref(out)),
-               "acForcingParamsGenerate")
-        return out
-
     # --- reductions (device layer: RMS/RMS_EXP are raw sums) --------------
     def reduce_scal(self, rtype: int, handle: int, stream: int = 0) -> float:
         r = self.prec.real()
@@ -293,3 +267,31 @@ class Ensemble:
         _check(self.lib.acEnsembleAutoOptimize(self.handle,
                                                cache_path.encode() if cache_path else None),
                "acEnsembleAutoOptimize")
+
+
+def forcing_params_from_uniforms(flavour: str, info, u) -> object:
+    """acForcingParamsFromUniforms: the step's forcing from five draws in [0, 1]."""
+    prec = abi.PRECISIONS[flavour]
+    lib = library.load(flavour)
+    out = abi.forcing_type(prec)()
+    arr = (prec.real * 5)(*[float(x) for x in u])
+    _check(lib.acForcingParamsFromUniforms(info, arr, C.byref(out)), "acForcingParamsFromUniforms")
+    return out
+
+
+class ForcingGenerator:
+    """acForcingParamsGenerate: a reproducible stream of per-step forcing
+    parameters from a seed."""
+
+    def __init__(self, flavour: str, info, seed: int):
+        self.prec = abi.PRECISIONS[flavour]
+        self.lib = library.load(flavour)
+        self.info = info
+        self.state = C.c_ulonglong(seed)
+
+    def next(self):
+        out = abi.forcing_type(self.prec)()
+        _check(self.lib.acForcingParamsGenerate(self.info, C.byref(self.state), C.byref(out)),
+               "acForcingParamsGenerate")
+        return out
+

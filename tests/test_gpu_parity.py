@@ -318,6 +318,45 @@ def test_forcing_vs_oracle(flavour):
     assert max(errs) <= TOL[flavour], errs
 
 
+@pytest.mark.parametrize("flavour", FLAVOURS)
+def test_generated_forcing_each_step_vs_oracle(flavour):
+    """Every step a new forcing from the seeded generator, loaded with
+    acDeviceLoadForcingParams (the reference standalone's per-step
+    generateForcingParams + loadForcingParamsToDevice); the oracle steps with
+    the same parameters."""
+    from astaroth_b200.device import ForcingGenerator
+
+    prec = abi.PRECISIONS[flavour]
+    n, steps = 24, 3
+    info = workload_info(prec, n, kmin=1.0, kmax=3.0, relhel=0.5, forcing_magnitude=0.05)
+    fields = init.workload_fields(n, n, n, prec.np_dtype, seed=21, amplitude=1e-3)
+    host = abi.HostMesh(prec, info, [f.copy() for f in fields])
+    dt = float(prec.np_dtype(1e-3))
+    gen = ForcingGenerator(flavour, info, seed=77)
+    params = [gen.next() for _ in range(steps)]
+    with new_device(flavour, info) as dev:
+        dev.set_forcing(True)
+        dev.load_mesh(host)
+        for fp in params:
+            dev.load_forcing_params(fp)
+            dev.integrate_step(dt)
+        dev.synchronize()
+        assert dev.status() == 0
+        out = [dev.store_double(w) for w in range(8)]
+    om = O.OracleMesh("f80", fields, n, n, n)
+    for fp in params:
+        p = O.params_from(info, forcing=1, forcing_magnitude=fp.magnitude,
+                          forcing_phase=fp.phase, kaver=fp.kaver, k_force=list(fp.k_force),
+                          ff_re=list(fp.ff_hel_re), ff_im=list(fp.ff_hel_im))
+        om.step(p, dt, 1)
+    errs = [O.normwise_error(interior(out[w]), om.interior(w)) for w in range(8)]
+    assert max(errs) <= TOL[flavour], errs
+    # the forcing moved the velocity well beyond the tolerance
+    free = O.OracleMesh("f80", fields, n, n, n)
+    free.step(O.params_from(info), dt, steps)
+    assert O.normwise_error(free.interior(1), om.interior(1)) > 100 * TOL[flavour]
+
+
 def test_mixed_tracks_fp64():
     """The mixed state stays close to the FP64 GPU path (64^3, 10 steps)."""
     n, steps, dt = 64, 10, float(np.float32(1e-3))
