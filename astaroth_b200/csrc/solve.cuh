@@ -398,6 +398,247 @@ field_derivs_q(const state_t* __restrict__ c, const int* zo, const SolveParams<T
     return r;
 }
 
+// ---- pairs of fields in packed FP32 lanes ----------------------------------
+// add/sub.rn.f32x2 operate on two independent FP32 lanes with the rounding of
+// the scalar operations, so a pair of fields whose stencils have the same
+// shape forms its sums and differences in half the instructions, bit for bit
+// as one field at a time.
+struct F2 {
+    unsigned long long v;
+};
+
+__device__ __forceinline__ F2
+pk2(float a, float b)
+{
+    F2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+    return r;
+}
+
+__device__ __forceinline__ void
+upk2(F2 r, float& a, float& b)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r.v));
+}
+
+__device__ __forceinline__ F2
+add2(F2 a, F2 b)
+{
+    F2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+
+__device__ __forceinline__ F2
+sub2(F2 a, F2 b)
+{
+    F2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+
+template <bool GX_, bool GY_, bool GZ_, bool XY_, bool XZ_, bool YZ_>
+struct DFlags {
+    static constexpr bool GX = GX_, GY = GY_, GZ = GZ_, XY = XY_, XZ = XZ_, YZ = YZ_;
+};
+
+// Upper half of a z-diagonal cross derivative (XK: xz, else yz) of one lane:
+// the ring offsets of its two points at plane z+k and its queued lower half.
+template <bool XK, int BX>
+struct ZCross {
+    static constexpr int step = XK ? 1 : BX;
+    __device__ __forceinline__ static float past(const ZQueue<float>& Q, int k)
+    {
+        return XK ? (k == 1 ? Q.x1 : (k == 2 ? Q.x2b : Q.x3c))
+                  : (k == 1 ? Q.y1 : (k == 2 ? Q.y2b : Q.y3c));
+    }
+};
+
+// Two z-diagonal cross derivatives (one of field A, kind XA; one of field B,
+// kind XB) with their differences formed in packed lanes.
+template <bool XA, bool XB, int BX>
+__device__ __forceinline__ void
+zcross_pair(const float* __restrict__ cA, const float* __restrict__ cB, const int* zo,
+            const SolveParams<float>& P, const ZQueue<float>& QA, const ZQueue<float>& QB,
+            float& sA, float& sB)
+{
+    using CA = ZCross<XA, BX>;
+    using CB = ZCross<XB, BX>;
+    float a[3], b[3];
+#pragma unroll
+    for (int k = 1; k <= 3; ++k) {
+        const int z  = zo[3 + k];
+        const F2 u   = sub2(pk2(cA[z + k * CA::step], cB[z + k * CB::step]),
+                            pk2(cA[z - k * CA::step], cB[z - k * CB::step]));
+        const F2 w   = sub2(u, pk2(CA::past(QA, k), CB::past(QB, k)));
+        upk2(w, a[k - 1], b[k - 1]);
+    }
+    const int ra = XA ? 1 : 2, rb = XB ? 1 : 2;
+    float s = P.cx[ra][0] * a[0];
+    s += P.cx[ra][1] * a[1];
+    s += P.cx[ra][2] * a[2];
+    sA = s;
+    float t = P.cx[rb][0] * b[0];
+    t += P.cx[rb][1] * b[1];
+    t += P.cx[rb][2] * b[2];
+    sB = t;
+}
+
+// One z-diagonal cross derivative of one field (no partner).
+template <bool XK, int BX>
+__device__ __forceinline__ float
+zcross_one(const float* __restrict__ c, const int* zo, const SolveParams<float>& P,
+           const ZQueue<float>& Q)
+{
+    using CK = ZCross<XK, BX>;
+    const int r = XK ? 1 : 2;
+    float s     = 0;
+#pragma unroll
+    for (int k = 1; k <= 3; ++k) {
+        const int z   = zo[3 + k];
+        const float u = c[z + k * CK::step] - c[z - k * CK::step];
+        s += P.cx[r][k - 1] * (u - CK::past(Q, k));
+    }
+    return s;
+}
+
+// Advances a single-precision queue by one plane (after every use of it).
+template <bool XZ, bool YZ>
+__device__ __forceinline__ void
+push_queue(ZQueue<float>& Q, float f0, const float* dx, const float* dy)
+{
+    if (XZ) {
+        Q.x3c = Q.x3b;
+        Q.x3b = Q.x3a;
+        Q.x3a = dx[2];
+        Q.x2b = Q.x2a;
+        Q.x2a = dx[1];
+        Q.x1  = dx[0];
+    }
+    if (YZ) {
+        Q.y3c = Q.y3b;
+        Q.y3b = Q.y3a;
+        Q.y3a = dy[2];
+        Q.y2b = Q.y2a;
+        Q.y2a = dy[1];
+        Q.y1  = dy[0];
+    }
+    Q.v3 = Q.v2;
+    Q.v2 = Q.v1;
+    Q.v1 = f0;
+}
+
+// field_derivs_q of two fields at once: every pencil sum and difference, the
+// xy diagonals both fields need and the paired z diagonals in packed lanes;
+// the coefficient sums per field exactly as field_derivs_q forms them.
+template <int BX, class FA, class FB>
+__device__ __forceinline__ void
+pair_derivs_q(const float* __restrict__ cA, const float* __restrict__ cB, const int* zo,
+              const SolveParams<float>& P, ZQueue<float>& QA, ZQueue<float>& QB,
+              FieldDerivs<float>& rA, FieldDerivs<float>& rB)
+{
+    const float a0 = cA[0], b0 = cB[0];
+    rA.v = a0;
+    rB.v = b0;
+    float dxA[3], dxB[3], sxA[3], sxB[3], dyA[3], dyB[3], syA[3], syB[3], dzA[3], dzB[3],
+        szA[3], szB[3];
+#pragma unroll
+    for (int k = 1; k <= 3; ++k) {
+        const F2 px = pk2(cA[k], cB[k]), mx = pk2(cA[-k], cB[-k]);
+        upk2(sub2(px, mx), dxA[k - 1], dxB[k - 1]);
+        upk2(add2(px, mx), sxA[k - 1], sxB[k - 1]);
+        const F2 py = pk2(cA[k * BX], cB[k * BX]), my = pk2(cA[-k * BX], cB[-k * BX]);
+        upk2(sub2(py, my), dyA[k - 1], dyB[k - 1]);
+        upk2(add2(py, my), syA[k - 1], syB[k - 1]);
+    }
+    {
+        const F2 p1 = pk2(cA[zo[4]], cB[zo[4]]), p2 = pk2(cA[zo[5]], cB[zo[5]]),
+                 p3 = pk2(cA[zo[6]], cB[zo[6]]);
+        const F2 m1 = pk2(QA.v1, QB.v1), m2 = pk2(QA.v2, QB.v2), m3 = pk2(QA.v3, QB.v3);
+        upk2(sub2(p1, m1), dzA[0], dzB[0]);
+        upk2(sub2(p2, m2), dzA[1], dzB[1]);
+        upk2(sub2(p3, m3), dzA[2], dzB[2]);
+        upk2(add2(p1, m1), szA[0], szB[0]);
+        upk2(add2(p2, m2), szA[1], szB[1]);
+        upk2(add2(p3, m3), szA[2], szB[2]);
+    }
+    auto first = [&](const float* c1, const float* d) { return c1[0] * d[0] + c1[1] * d[1] + c1[2] * d[2]; };
+    auto second = [&](const float* c2, float f0, const float* s) {
+        return c2[0] * f0 + c2[1] * s[0] + c2[2] * s[1] + c2[3] * s[2];
+    };
+    if (FA::GX) rA.gx = first(P.c1[0], dxA);
+    if (FB::GX) rB.gx = first(P.c1[0], dxB);
+    if (FA::GY) rA.gy = first(P.c1[1], dyA);
+    if (FB::GY) rB.gy = first(P.c1[1], dyB);
+    if (FA::GZ) rA.gz = first(P.c1[2], dzA);
+    if (FB::GZ) rB.gz = first(P.c1[2], dzB);
+    rA.xx = second(P.c2[0], a0, sxA);
+    rB.xx = second(P.c2[0], b0, sxB);
+    rA.yy = second(P.c2[1], a0, syA);
+    rB.yy = second(P.c2[1], b0, syB);
+    rA.zz = second(P.c2[2], a0, szA);
+    rB.zz = second(P.c2[2], b0, szB);
+
+    // xy diagonals (the whole stencil from the centre plane)
+    if (FA::XY || FB::XY) {
+        float eA[3], eB[3];
+#pragma unroll
+        for (int k = 1; k <= 3; ++k) {
+            const int pp = k + k * BX, mm = -k - k * BX, pm = k - k * BX, mp = -k + k * BX;
+            if (FA::XY && FB::XY) {
+                const F2 a = add2(pk2(cA[pp], cB[pp]), pk2(cA[mm], cB[mm]));
+                const F2 b = add2(pk2(cA[pm], cB[pm]), pk2(cA[mp], cB[mp]));
+                upk2(sub2(a, b), eA[k - 1], eB[k - 1]);
+            }
+            else if (FA::XY) {
+                eA[k - 1] = (cA[pp] + cA[mm]) - (cA[pm] + cA[mp]);
+            }
+            else {
+                eB[k - 1] = (cB[pp] + cB[mm]) - (cB[pm] + cB[mp]);
+            }
+        }
+        if (FA::XY) {
+            float s = 0;
+            s += P.cx[0][0] * eA[0];
+            s += P.cx[0][1] * eA[1];
+            s += P.cx[0][2] * eA[2];
+            rA.xy = s;
+        }
+        if (FB::XY) {
+            float s = 0;
+            s += P.cx[0][0] * eB[0];
+            s += P.cx[0][1] * eB[1];
+            s += P.cx[0][2] * eB[2];
+            rB.xy = s;
+        }
+    }
+
+    // z diagonals: the first of A's with the first of B's, the second with the second
+    constexpr int nA = (FA::XZ ? 1 : 0) + (FA::YZ ? 1 : 0);
+    constexpr int nB = (FB::XZ ? 1 : 0) + (FB::YZ ? 1 : 0);
+    constexpr bool A1X = FA::XZ, B1X = FB::XZ; // kind of each field's first z diagonal
+    float zA[2] = {0, 0}, zB[2] = {0, 0};
+    if constexpr (nA >= 1 && nB >= 1)
+        zcross_pair<A1X, B1X, BX>(cA, cB, zo, P, QA, QB, zA[0], zB[0]);
+    else if constexpr (nA >= 1)
+        zA[0] = zcross_one<A1X, BX>(cA, zo, P, QA);
+    else if constexpr (nB >= 1)
+        zB[0] = zcross_one<B1X, BX>(cB, zo, P, QB);
+    if constexpr (nA == 2 && nB == 2)
+        zcross_pair<false, false, BX>(cA, cB, zo, P, QA, QB, zA[1], zB[1]);
+    else if constexpr (nA == 2)
+        zA[1] = zcross_one<false, BX>(cA, zo, P, QA);
+    else if constexpr (nB == 2)
+        zB[1] = zcross_one<false, BX>(cB, zo, P, QB);
+    if (FA::XZ) rA.xz = zA[0];
+    if (FA::YZ) rA.yz = FA::XZ ? zA[1] : zA[0];
+    if (FB::XZ) rB.xz = zB[0];
+    if (FB::YZ) rB.yz = FB::XZ ? zB[1] : zB[0];
+
+    push_queue<FA::XZ, FA::YZ>(QA, a0, dxA, dyA);
+    push_queue<FB::XZ, FB::YZ>(QB, b0, dxB, dyB);
+}
+
 // Derivative flags of the eight fields: what the right-hand sides use.
 //                   GX     GY     GZ     XY     XZ     YZ
 #define ACB_D_LNRHO true, true, true, false, false, false
@@ -440,15 +681,30 @@ __device__ __forceinline__ void
 mhd_rhs_q(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, T roc[ACB_NF],
           T cur[ACB_NF], ZQueue<T> (&Q)[ACB_NF])
 {
-    const auto lr = field_derivs_q<T, BX, ACB_D_LNRHO>(c + 0 * FIELD, zo, P, Q[0]);
-    const auto ux = field_derivs_q<T, BX, ACB_D_UUX>(c + 1 * FIELD, zo, P, Q[1]);
-    const auto uy = field_derivs_q<T, BX, ACB_D_UUY>(c + 2 * FIELD, zo, P, Q[2]);
-    const auto uz = field_derivs_q<T, BX, ACB_D_UUZ>(c + 3 * FIELD, zo, P, Q[3]);
-    const auto ax = field_derivs_q<T, BX, ACB_D_AX>(c + 4 * FIELD, zo, P, Q[4]);
-    const auto ay = field_derivs_q<T, BX, ACB_D_AY>(c + 5 * FIELD, zo, P, Q[5]);
-    const auto az = field_derivs_q<T, BX, ACB_D_AZ>(c + 6 * FIELD, zo, P, Q[6]);
-    const auto ss = field_derivs_q<T, BX, ACB_D_SS>(c + 7 * FIELD, zo, P, Q[7]);
-    rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
+    if constexpr (sizeof(T) == 4 && sizeof(state_t) == 4) {
+        // in pairs of like-shaped stencils, two packed lanes per instruction
+        FieldDerivs<T> lr, ux, uy, uz, ax, ay, az, ss;
+        pair_derivs_q<BX, DFlags<ACB_D_LNRHO>, DFlags<ACB_D_SS>>(c + 0 * FIELD, c + 7 * FIELD, zo,
+                                                                 P, Q[0], Q[7], lr, ss);
+        pair_derivs_q<BX, DFlags<ACB_D_UUX>, DFlags<ACB_D_UUY>>(c + 1 * FIELD, c + 2 * FIELD, zo,
+                                                                P, Q[1], Q[2], ux, uy);
+        pair_derivs_q<BX, DFlags<ACB_D_AX>, DFlags<ACB_D_AY>>(c + 4 * FIELD, c + 5 * FIELD, zo, P,
+                                                              Q[4], Q[5], ax, ay);
+        pair_derivs_q<BX, DFlags<ACB_D_UUZ>, DFlags<ACB_D_AZ>>(c + 3 * FIELD, c + 6 * FIELD, zo,
+                                                               P, Q[3], Q[6], uz, az);
+        rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
+    }
+    else {
+        const auto lr = field_derivs_q<T, BX, ACB_D_LNRHO>(c + 0 * FIELD, zo, P, Q[0]);
+        const auto ux = field_derivs_q<T, BX, ACB_D_UUX>(c + 1 * FIELD, zo, P, Q[1]);
+        const auto uy = field_derivs_q<T, BX, ACB_D_UUY>(c + 2 * FIELD, zo, P, Q[2]);
+        const auto uz = field_derivs_q<T, BX, ACB_D_UUZ>(c + 3 * FIELD, zo, P, Q[3]);
+        const auto ax = field_derivs_q<T, BX, ACB_D_AX>(c + 4 * FIELD, zo, P, Q[4]);
+        const auto ay = field_derivs_q<T, BX, ACB_D_AY>(c + 5 * FIELD, zo, P, Q[5]);
+        const auto az = field_derivs_q<T, BX, ACB_D_AZ>(c + 6 * FIELD, zo, P, Q[6]);
+        const auto ss = field_derivs_q<T, BX, ACB_D_SS>(c + 7 * FIELD, zo, P, Q[7]);
+        rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
+    }
 }
 
 template <typename T, int BX, int FIELD>
