@@ -401,6 +401,58 @@ def test_reference_ctest_sample_runs(tmp_path):
     assert "FAIL" not in r.stdout
 
 
+def test_reference_standalone_simulation_runs_and_matches_oracle(tmp_path):
+    """The reference's standalone sample (samples/standalone, sources unchanged,
+    linked against the FP32 library) runs its simulation mode: Legacy API steps
+    with the host CFL time step, diagnostics every step into timeseries.ts and
+    .mesh snapshots at steps 0 and 4. The oracle, started from the step-0
+    snapshot and stepped with the time steps the sample reports, must reproduce
+    the step-4 snapshot, and the sample's max|u| must be that of the snapshot."""
+    exe = os.path.join(abi.REPO, "oracle", "_ref", "ac_run_sp")
+    if not os.path.exists(exe):
+        pytest.skip("standalone binary not built (needs the reference sources at build time)")
+    n, steps = 24, 4
+    cfg = dict(abi.DEFAULT_CONFIG)
+    cfg.update({"AC_nx": n, "AC_ny": n, "AC_nz": n, "AC_dsx": 2 * math.pi / n,
+                "AC_dsy": 2 * math.pi / n, "AC_dsz": 2 * math.pi / n,
+                "AC_max_steps": steps + 1, "AC_save_steps": 1, "AC_bin_steps": steps,
+                "AC_bin_save_t": "1e666"})
+    conf = tmp_path / "sim.conf"
+    conf.write_text("".join(f"{k} = {v}\n" for k, v in cfg.items()))
+    r = subprocess.run([exe, "--simulate", "--config", str(conf)], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    m = n + 6
+
+    def snapshot(step):
+        out = []
+        for name in abi.VTXBUFS:
+            raw = np.fromfile(tmp_path / f"{name}_{step}.mesh", dtype=np.float32)
+            assert raw.size == 1 + m ** 3, name
+            out.append(raw[1:].reshape(m, m, m).astype(np.float64))
+        return float(raw[0]), out
+
+    t0, s0 = snapshot(0)
+    t4, s4 = snapshot(steps)
+    rows = [ln.split() for ln in (tmp_path / "timeseries.ts").read_text().splitlines()[1:] if ln.strip()]
+    dts = {int(row[0]): float(row[2]) for row in rows}
+    assert sorted(dts) == list(range(steps + 1))
+    assert all(np.isfinite(f).all() for f in s4)
+    assert t4 == pytest.approx(sum(dts[i] for i in range(1, steps + 1)), rel=1e-5)
+
+    info = abi.make_info(abi.SP, n, **{k: v for k, v in cfg.items() if k in abi.REAL_PARAMS
+                                       and k not in ("AC_bin_save_t",)})
+    p = O.params_from(info)
+    om = O.OracleMesh("f80", [np.ascontiguousarray(f) for f in s0], n, n, n)
+    for i in range(1, steps + 1):
+        om.step(p, dts[i], 1)
+    errs = [O.normwise_error(interior(s4[w]), om.interior(w)) for w in range(8)]
+    assert max(errs) <= TOL["sp"], errs
+    umax_sample = float(rows[-1][5])
+    umax_snap = np.max(np.sqrt(sum(interior(s4[c]) ** 2 for c in (1, 2, 3))))
+    assert umax_sample == pytest.approx(umax_snap, rel=1e-5)
+
+
 @pytest.mark.parametrize("flavour", FLAVOURS)
 @pytest.mark.parametrize("dims", [(20, 14, 11), (131, 5, 4), (7, 4, 5)])
 def test_whole_box_fill_after_substep_is_exact(flavour, dims):
