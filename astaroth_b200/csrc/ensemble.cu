@@ -153,10 +153,27 @@ build_tables(Ensemble e)
         D.assign(n, MemberDesc<AcReal>());
         std::vector<HaloMember> H(n);
         long long tasks = 0, units = 0;
-        for (int i = 0; i < n; ++i) {
+        // Task list order: members with the longest tasks (z segment + halo
+        // planes) first, so that the persistent CTAs, which take tasks
+        // round-robin, finish the launch on short tasks instead of idling
+        // behind a few long ones (longest-processing-time-first).
+        auto zseg_of = [&](const Layout& L) {
+            int nseg = 1;
+            if (e->seg_planes > 0)
+                nseg = std::max(1, (int)lround((double)L.nz / e->seg_planes));
+            return (L.nz + nseg - 1) / nseg;
+        };
+        std::vector<int> order(n);
+        for (int i = 0; i < n; ++i)
+            order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return zseg_of(e->m[a].L) > zseg_of(e->m[b].L);
+        });
+        for (int pos = 0; pos < n; ++pos) {
+            const int i      = order[pos];
             const Member& mb = e->m[i];
             const Layout& L  = mb.L;
-            MemberDesc<AcReal>& d = D[i];
+            MemberDesc<AcReal>& d = D[pos];
             memset(&d, 0, sizeof(d));
             if (encode_block_map(L, mb.blk[p], cfg, &d.tmap) != AC_SUCCESS)
                 return AC_FAILURE;
@@ -168,10 +185,7 @@ build_tables(Ensemble e)
             g.ntx        = (L.nx + cfg.TX - 1) / cfg.TX;
             g.nty        = (L.ny + cfg.TY - 1) / cfg.TY;
             g.nzr        = L.nz;
-            int nseg     = 1;
-            if (e->seg_planes > 0)
-                nseg = std::max(1, (int)lround((double)L.nz / e->seg_planes));
-            g.zseg        = (L.nz + nseg - 1) / nseg;
+            g.zseg        = zseg_of(L);
             g.nseg        = (L.nz + g.zseg - 1) / g.zseg;
             g.tasks       = (long long)g.ntx * g.nty * g.nseg;
             d.task_begin  = tasks;
@@ -180,11 +194,11 @@ build_tables(Ensemble e)
             d.in_lo       = mb.lo[p];
             d.out_lo      = mb.lo[p ^ 1];
             d.P           = make_params(mb.uniforms, L, 0, 0);
-            H[i].L         = L;
-            H[i].block     = mb.blk[p];
-            H[i].lo        = mb.lo[p];
-            H[i].unit_begin = units;
-            H[i].units_a    = (unsigned)halo_units_a(L);
+            H[pos].L          = L;
+            H[pos].block      = mb.blk[p];
+            H[pos].lo         = mb.lo[p];
+            H[pos].unit_begin = units;
+            H[pos].units_a    = (unsigned)halo_units_a(L);
             units += halo_units(L);
         }
         e->total_tasks = tasks;
