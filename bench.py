@@ -16,8 +16,9 @@ acDeviceIntegrateSubstep, acDeviceSwapBuffers). Inputs are larger than L2
 
 Beside the headline line: the FP64 and FP32 libraries on the same steps (and
 the per-field error against FP64), an end-to-end run from pinned host memory,
-the 64-member ensemble, and the forced large-mesh run (1024^3 mixed, helical
-forcing from a seeded generator and four FP64 diagnostics every step).
+the 64-member ensemble, the 256^3 FP32 and FP64 runs with four reductions read
+back every step, and the forced large-mesh run (1024^3 mixed, helical forcing
+from a seeded generator and four FP64 diagnostics every step).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -61,6 +62,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-forced", action="store_true",
                     help="skip the forced large-mesh run (helical forcing + diagnostics)")
     ap.add_argument("--forced-n", type=int, default=1024, help="mesh size of the forced run")
+    ap.add_argument("--no-diagnostics", action="store_true",
+                    help="skip the 256^3 FP32/FP64 run with reductions every step")
     return ap.parse_args(argv)
 
 
@@ -514,6 +517,57 @@ def forced_run(n: int, steps: int, warmup: int, ranks, gpu: int) -> dict:
         torch.cuda.empty_cache()
 
 
+def diagnostics_run(n: int, steps: int, warmup: int, ranks, gpu: int) -> dict:
+    """The diagnostics workload: an n^3 mesh (256^3) of the seeded state in
+    FP32 and in FP64, each step an RK3 step followed by max, min and rms of |u|
+    and rms_exp of lnrho, each read back (FP64 accumulation); reported as
+    step-only time, step + diagnostics time and the time of one reduction."""
+    import torch
+
+    from astaroth_b200 import Device, abi
+
+    out = {"mesh": [n, n, n], "steps": steps, "warmup": warmup,
+           "diagnostics": "max, min, rms of |u|; rms_exp of lnrho; each read back"}
+    for flav in ("sp", "dp"):
+        host = host_mesh(flav, n)
+        dev = Device(flav, host.info, gpu)
+        try:
+            dev.load_mesh(host)
+            st = torch.cuda.ExternalStream(dev.cuda_stream(0))
+
+            def diag():
+                dev.reduce_vec(abi.RTYPE_MAX, abi.VTXBUF_UUX, abi.VTXBUF_UUY, abi.VTXBUF_UUZ)
+                dev.reduce_vec(abi.RTYPE_MIN, abi.VTXBUF_UUX, abi.VTXBUF_UUY, abi.VTXBUF_UUZ)
+                dev.reduce_vec(abi.RTYPE_RMS, abi.VTXBUF_UUX, abi.VTXBUF_UUY, abi.VTXBUF_UUZ)
+                dev.reduce_scal(abi.RTYPE_RMS_EXP, abi.VTXBUF_LNRHO)
+
+            def timed(fn, k):
+                for _ in range(warmup):
+                    fn()
+                dev.synchronize()
+                ranks.barrier()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                for _ in range(k):
+                    fn()
+                e1.record(st)
+                e1.synchronize()
+                return ranks.max(e0.elapsed_time(e1)) / k
+
+            step_ms = timed(lambda: dev.integrate_step(DT), steps)
+            both_ms = timed(lambda: (dev.integrate_step(DT), diag()), steps)
+            red_ms = timed(diag, steps) / 4
+            out[flav] = {"ms_per_step": step_ms, "ms_per_step_with_diagnostics": both_ms,
+                         "ms_per_reduction": red_ms,
+                         "cell_updates_per_s_with_diagnostics":
+                             ranks.world * n ** 3 / (both_ms * 1e-3)}
+        finally:
+            dev.destroy()
+            del host
+            torch.cuda.empty_cache()
+    return out
+
+
 def profile_traffic(name: str):
     """Per-launch DRAM bytes of the dominant kernel from a committed ncu
     summary (a line `traffic_bytes_per_launch: <value>`), else None."""
@@ -635,6 +689,10 @@ def run_ours(args) -> None:
     if not args.no_ensemble:
         ensemble = ensemble_run(min(args.steps, 20), ranks)
 
+    diagnostics = None
+    if not args.no_diagnostics:
+        diagnostics = diagnostics_run(256, 100, max(args.warmup, 3), ranks, gpu)
+
     forced = None
     if not args.no_forced:
         torch.cuda.empty_cache()
@@ -659,7 +717,7 @@ def run_ours(args) -> None:
                              "solve_ms_per_substep": res["solve_ms_per_substep"]},
                 "clocks": res["clocks"], "gpu_launches": res["launches"],
                 "e2e": e2e, "cpu_baseline": cpu, "variants": variants, "errors": errors,
-                "ensemble": ensemble, "forced": forced}
+                "ensemble": ensemble, "diagnostics_256": diagnostics, "forced": forced}
         print(json.dumps(line), flush=True)
     ranks.close()
 
