@@ -52,6 +52,8 @@ NUM_REAL_PARAMS = len(REAL_PARAMS)
 NUM_REAL3_PARAMS = len(REAL3_PARAMS)
 NUM_VTXBUF_HANDLES = len(VTXBUFS)
 AC_SUCCESS, AC_FAILURE = 0, 1
+# include/astaroth.h AcBoundcond
+AC_BOUNDCOND_PERIODIC, AC_BOUNDCOND_SYMMETRIC, AC_BOUNDCOND_ANTISYMMETRIC = 0, 1, 2
 
 
 class int3(C.Structure):

@@ -1149,15 +1149,49 @@ acDeviceGeneralBoundcondStep(const Device device, const Stream stream,
                              const VertexBufferHandle h, const int3 start, const int3 end,
                              const AcMeshInfo config, const int3 bindex)
 {
-    (void)bindex;
-    // The reference dispatches on the x-top condition only
-    // (src/core/kernels/boundconds.cuh:192-242); its symmetric kernels write
-    // sign*src*0 + 1 (:127) and are not reproduced.
+    (void)bindex; // the reference mirrors only for bindex.x < 0, which its Node always passes
+    // As the reference (src/core/kernels/boundconds.cuh:192-242), the x-top
+    // condition selects the fill of every face.
     const int bc = config.int_params[AC_bc_type_top_x];
     if (bc == AC_BOUNDCOND_PERIODIC)
         return acDevicePeriodicBoundcondStep(device, stream, h, start, end);
-    fprintf(stderr, "ERROR: Boundary condition %d not supported (periodic only)\n", bc);
-    return AC_FAILURE;
+    if (bc != AC_BOUNDCOND_SYMMETRIC && bc != AC_BOUNDCOND_ANTISYMMETRIC) {
+        fprintf(stderr, "ERROR: Boundary condition not recognized! (%d)\n", bc);
+        return AC_FAILURE;
+    }
+    if (h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    cudaSetDevice(device->id);
+    const Layout& L = device->L;
+    if (L.nx < NGHOST + 1 || L.ny < NGHOST + 1 || L.nz < NGHOST + 1) {
+        fprintf(stderr, "astaroth_b200: symmetric boundaries need n >= 4 on every axis\n");
+        return AC_FAILURE;
+    }
+    int3 s = start, e = end;
+    s.x = std::max(s.x, 0);
+    s.y = std::max(s.y, 0);
+    s.z = std::max(s.z, 0);
+    e.x = std::min(e.x, L.mx);
+    e.y = std::min(e.y, L.my);
+    e.z = std::min(e.z, L.mz);
+    if (e.x <= s.x || e.y <= s.y || e.z <= s.z)
+        return AC_SUCCESS;
+    HaloArgs a;
+    a.L     = L;
+    a.block = device->blk[device->cur];
+    a.lo    = device->lo[device->cur];
+    a.start = s;
+    a.end   = e;
+    a.f0    = (int)h;
+    a.f1    = (int)h + 1;
+    a.rows  = (long long)(e.y - s.y) * (e.z - s.z);
+    const long long blocks = std::min((a.rows + 7) / 8, (long long)device->num_sms * 16);
+    mirror_kernel<<<(unsigned)blocks, 256, 0, stream_of(device, stream)>>>(
+        a, bc == AC_BOUNDCOND_SYMMETRIC ? 1.0f : -1.0f);
+    ACB_CUDA_CHECK(cudaGetLastError());
+    device->launches++;
+    device->ghost_ok[device->cur] = false; // no longer the periodic images
+    return AC_SUCCESS;
 }
 
 AcResult

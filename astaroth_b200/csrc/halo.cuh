@@ -283,3 +283,49 @@ halo_batch_kernel(const HaloMember* __restrict__ mem, int n, long long total_uni
         halo_unit(m.L, m.block, m.lo, m.units_a, (unsigned)(u - m.unit_begin));
     }
 }
+
+// ---------------------------------------------------------------------------
+// Symmetric / antisymmetric ghost fill (reference src/core/kernels/
+// boundconds.cuh:3-128 as intended): every ghost vertex takes sign times the
+// vertex mirrored about the first or last interior point on each axis where
+// it lies outside the interior, c' = 2 * 3 - c below and 2 * (n + 2) - c
+// above (vertex-centred walls), the sign applied once (+1 symmetric, -1
+// antisymmetric). The reference kernel writes sign * src * 0 + 1 instead
+// (:127) and compares y against the x bound (:62, :93); both are corrected.
+// With n >= 4 on every axis every source is an interior vertex, so all
+// writes are independent.
+__device__ __forceinline__ int
+mirror_interior(int c, int n)
+{
+    return c < NGHOST ? 2 * NGHOST - c : (c > n + NGHOST - 1 ? 2 * (n + NGHOST - 1) - c : c);
+}
+
+static __global__ void __launch_bounds__(256)
+mirror_kernel(const HaloArgs a, const float sign)
+{
+    const int lane         = threadIdx.x & 31;
+    const long long warp   = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const Layout& L        = a.L;
+    const int ry           = a.end.y - a.start.y;
+    for (long long r = warp; r < a.rows; r += nwarps) {
+        const int j          = a.start.y + (int)(r % ry);
+        const int k          = a.start.z + (int)(r / ry);
+        const bool ghost_row = j < NGHOST || j >= NGHOST + L.ny || k < NGHOST || k >= NGHOST + L.nz;
+        const long long drow = lidx(L, 0, j, k);
+        const long long srow = lidx(L, 0, mirror_interior(j, L.ny), mirror_interior(k, L.nz));
+        for (int i = a.start.x + lane; i < a.end.x; i += 32) {
+            if (!ghost_row && i >= NGHOST && i < NGHOST + L.nx)
+                continue; // interior vertex
+            const int is = mirror_interior(i, L.nx);
+            for (int f = a.f0; f < a.f1; ++f) {
+                state_t* F                         = a.block + f * L.fstride;
+                F[drow + i]                        = (state_t)sign * F[srow + is];
+                if (ACB_MIXED && a.lo) {
+                    float* G    = a.lo + f * L.fstride;
+                    G[drow + i] = sign * G[srow + is];
+                }
+            }
+        }
+    }
+}

@@ -125,6 +125,8 @@ def _declare(lib: C.CDLL, prec: abi.Precision) -> None:
         # legacy
         "acInit": (res, [Info]),
         "acQuit": (res, []),
+        "acIntegrateGBC": (res, [Info, R]),
+        "acBoundcondStepGBC": (res, [Info]),
         "acLoad": (res, [Mesh]),
         "acStore": (res, [C.POINTER(Mesh)]),
         "acIntegrate": (res, [R]),

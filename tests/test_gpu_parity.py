@@ -401,6 +401,89 @@ def test_reference_ctest_sample_runs(tmp_path):
     assert "FAIL" not in r.stdout
 
 
+def mirror_fill_numpy(a, sign):
+    """Restatement of the symmetric/antisymmetric fill as the reference intends it
+    (src/core/kernels/boundconds.cuh:3-128): each ghost vertex takes sign times
+    the vertex mirrored about the first/last interior point on every axis where
+    it lies outside the interior."""
+    g = abi.NGHOST
+    out = a.copy()
+    mz, my, mx = a.shape
+
+    def mir(c, m):
+        n = m - 2 * g
+        return 2 * g - c if c < g else (2 * (n + g - 1) - c if c > n + g - 1 else c)
+
+    for k in range(mz):
+        for j in range(my):
+            for i in range(mx):
+                if g <= i < mx - g and g <= j < my - g and g <= k < mz - g:
+                    continue
+                out[k, j, i] = sign * a[mir(k, mz), mir(j, my), mir(i, mx)]
+    return out
+
+
+@pytest.mark.parametrize("flavour", FLAVOURS)
+@pytest.mark.parametrize("bc", [abi.AC_BOUNDCOND_SYMMETRIC, abi.AC_BOUNDCOND_ANTISYMMETRIC])
+def test_symmetric_boundaries_exact(flavour, bc):
+    """acDeviceGeneralBoundconds with a symmetric or antisymmetric condition
+    (selected by AC_bc_type_top_x, as in the reference): ghosts equal sign
+    times the mirrored interior, bit for bit, on a non-cubic mesh; the interior
+    is untouched; a later periodic fill is not skipped."""
+    prec = abi.PRECISIONS[flavour]
+    nx, ny, nz = 9, 7, 5
+    info = workload_info(prec, nx, ny, nz, bc_type_top_x=bc)
+    fields = init.workload_fields(nx, ny, nz, prec.np_dtype, seed=31, amplitude=0.5)
+    host = abi.HostMesh(prec, info, [f.copy() for f in fields])
+    sign = 1.0 if bc == abi.AC_BOUNDCOND_SYMMETRIC else -1.0
+    with new_device(flavour, info) as dev:
+        dev.load_mesh(host)
+        dev.periodic_boundconds()  # the ghosts hold periodic images first
+        s, e = dev.full_box()
+        rc = dev.lib.acDeviceGeneralBoundconds(dev.handle, 0, s, e, info, abi.int3(-1, -1, -1))
+        assert rc == abi.AC_SUCCESS
+        got = [dev.store_double(w) for w in range(8)]
+        dev.periodic_boundconds()  # must run again: the ghosts are mirror images now
+        back = [dev.store_double(w) for w in range(8)]
+    for w in range(8):
+        want = mirror_fill_numpy(fields[w].astype(np.float64), sign)
+        assert np.array_equal(got[w], want), w
+        assert np.array_equal(back[w], init.wrap_ghosts(interior(fields[w].astype(np.float64)))), w
+
+
+def test_symmetric_boundaries_through_legacy_integrate():
+    """acIntegrateGBC with a symmetric condition (the standalone's integration
+    call) equals the Device sequence general fill + substep + swap, bit for bit."""
+    prec = abi.SP
+    n = 12
+    info = workload_info(prec, n, bc_type_top_x=abi.AC_BOUNDCOND_SYMMETRIC)
+    fields = init.workload_fields(n, n, n, np.float32, seed=32, amplitude=0.01)
+    dt = float(np.float32(1e-3))
+    with new_device("sp", info) as dev:
+        dev.load_mesh(abi.HostMesh(prec, info, [f.copy() for f in fields]))
+        s, e = dev.full_box()
+        for step in range(3):
+            assert dev.lib.acDeviceGeneralBoundconds(dev.handle, 0, s, e, info,
+                                                     abi.int3(-1, -1, -1)) == abi.AC_SUCCESS
+            dev.integrate_substep(step, dt)
+            dev.swap_buffers()
+        dev.synchronize()
+        ref = [dev.store_double(w) for w in range(8)]
+    from astaroth_b200 import library
+
+    lib = library.load("sp")
+    assert lib.acInit(info) == 0
+    try:
+        assert lib.acLoad(abi.HostMesh(prec, info, [f.copy() for f in fields]).cmesh) == 0
+        assert lib.acIntegrateGBC(info, C.c_float(dt)) == 0
+        out = abi.HostMesh(prec, info)
+        assert lib.acStore(C.byref(out.cmesh)) == 0
+    finally:
+        lib.acQuit()
+    for w in range(8):
+        assert np.array_equal(interior(out.fields[w].astype(np.float64)), interior(ref[w])), w
+
+
 def test_reference_standalone_simulation_runs_and_matches_oracle(tmp_path):
     """The reference's standalone sample (samples/standalone, sources unchanged,
     linked against the FP32 library) runs its simulation mode: Legacy API steps
