@@ -71,10 +71,16 @@ def parse_args(argv=None):
 # ranks
 # ---------------------------------------------------------------------------
 class Ranks:
-    def __init__(self, gpus: int):
+    """One process per GPU (torchrun environment). Replicas only: the group is
+    used for the barrier around the timed region and the max of the timings,
+    never on the data path. backend "nccl" on GPUs; "gloo" runs the same logic
+    on CPU processes (tests)."""
+
+    def __init__(self, gpus: int, backend: str = "nccl"):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.dist = None
         if self.world > 1:
             import datetime
@@ -82,27 +88,39 @@ class Ranks:
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                    device_id=torch.device("cuda", self.local))
+            kw = {}
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                kw["device_id"] = torch.device("cuda", self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300), **kw)
             self.dist = dist
 
-    def barrier(self):
-        import torch
+    def _sync(self):
+        if self.backend == "nccl":
+            import torch
 
-        torch.cuda.synchronize()
+            torch.cuda.synchronize()
+
+    def barrier(self):
+        self._sync()
         if self.dist:
             self.dist.barrier()
-        torch.cuda.synchronize()
+        self._sync()
 
     def max(self, x: float) -> float:
         if not self.dist:
             return x
         import torch
 
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
+
+    def throughput(self, cells_per_rank: int, steps: int, ms: float) -> float:
+        """Whole-job cell updates per second: every rank's cells over the max
+        time (pass `ms` already reduced with max())."""
+        return self.world * cells_per_rank * steps / (ms * 1e-3)
 
     def close(self):
         if self.dist:
@@ -632,8 +650,7 @@ def run_ours(args) -> None:
     dev = Device("mixed", host.info, gpu)
     dev.load_mesh(host)
     res = timed_steps(dev, args.steps, args.warmup, ranks, sample_clocks=True, gpu_index=gpu)
-    cells = ranks.world * n ** 3 * args.steps
-    value = cells / (res["total_ms"] * 1e-3)
+    value = ranks.throughput(n ** 3, args.steps, res["total_ms"])  # total_ms: max over ranks
 
     # roofline of the dominant kernel (the fused solve): algorithmic bytes per
     # launch over the average launch time from the events around every launch
