@@ -66,6 +66,10 @@ struct device_s {
     // interior (set by a full-box fill of all fields; cleared by any write to
     // the block). A fill of a block whose ghosts are already valid is skipped.
     bool ghost_ok[2];
+    // lo_stale[b] (mixed build): the last whole-box fill of block b wrote the
+    // hi parts of its ghosts only (the stencils never read the lo parts); the
+    // lo parts are filled before anything reads or partly overwrites them
+    bool lo_stale[2];
 
     CUtensorMap tmap[2];
     CentreMaps cmap[2]; // by parity of `in`: centre boxes over out hi, in lo, out lo
@@ -91,6 +95,7 @@ struct device_s {
     unsigned long long graph_key[2];
     unsigned long long graph_launches[2];
     bool graph_ghost[2][2]; // ghost_ok of both blocks after a replay of graph[p]
+    bool graph_lo[2][2];    // lo_stale of both blocks after a replay of graph[p]
 };
 
 // ---------------------------------------------------------------------------
@@ -403,6 +408,27 @@ launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e)
     ACB_CUDA_CHECK(cudaGetLastError());
     d->launches++;
     d->ghost_ok[d->cur ^ 1] = false; // the out block's ghosts are stale now
+    d->lo_stale[d->cur ^ 1] = false; // (all of them, hi and lo alike)
+    return AC_SUCCESS;
+}
+
+// Fills the lo parts of block b's ghosts with their periodic images if the last
+// whole-box fill of b left them (see lo_stale): the lo block is a block of
+// floats with the same layout, filled like the hi parts.
+static AcResult
+ensure_lo_ghosts(const Device d, cudaStream_t st, int b)
+{
+    if (!d->lo[b] || !d->lo_stale[b])
+        return AC_SUCCESS;
+    const Layout& L       = d->L;
+    const long long units = halo_units(L);
+    const int blocks =
+        (int)std::max(1LL, std::min((units + 255) / 256, (long long)d->num_sms * 32));
+    halo_full_kernel<<<blocks, 256, 0, st>>>(L, reinterpret_cast<state_t*>(d->lo[b]), nullptr,
+                                             (unsigned)halo_units_a(L), (unsigned)units);
+    ACB_CUDA_CHECK(cudaGetLastError());
+    d->launches++;
+    d->lo_stale[b] = false;
     return AC_SUCCESS;
 }
 
@@ -426,13 +452,16 @@ launch_halo(const Device d, cudaStream_t st, int3 s, int3 e, int f0, int f1)
         const long long units = halo_units(L);
         const long long want  = (units + 255) / 256;
         const int blocks = (int)std::max(1LL, std::min(want, (long long)d->num_sms * 32));
-        halo_full_kernel<<<blocks, 256, 0, st>>>(L, d->blk[d->cur], d->lo[d->cur],
+        halo_full_kernel<<<blocks, 256, 0, st>>>(L, d->blk[d->cur], nullptr,
                                                  (unsigned)halo_units_a(L), (unsigned)units);
         ACB_CUDA_CHECK(cudaGetLastError());
         d->launches++;
         d->ghost_ok[d->cur] = true;
+        d->lo_stale[d->cur] = d->lo[d->cur] != nullptr;
         return AC_SUCCESS;
     }
+    if (ensure_lo_ghosts(d, st, d->cur) != AC_SUCCESS)
+        return AC_FAILURE;
     HaloArgs a;
     a.L     = L;
     a.block = d->blk[d->cur];
@@ -579,6 +608,8 @@ launch_pack(const Device d, cudaStream_t st, int blk, int handle, double* flat, 
             int fill, double value)
 {
     const Layout& L = d->L;
+    if (ensure_lo_ghosts(d, st, blk) != AC_SUCCESS)
+        return AC_FAILURE;
     state_t* f      = d->blk[blk] + handle * L.fstride;
     float* lo       = d->lo[blk] ? d->lo[blk] + handle * L.fstride : nullptr;
     pack_kernel<<<d->num_sms * 8, 256, 0, st>>>(L, f, lo, flat, to_flat, fill, value);
@@ -944,6 +975,8 @@ acDeviceLoadVertexBufferWithOffset(const Device device, const Stream stream,
     const Layout& L   = device->L;
     float* lo         = device->lo[device->cur] ? device->lo[device->cur] + h * L.fstride : nullptr;
     device->ghost_ok[device->cur] = false;
+    if (ensure_lo_ghosts(device, stream_of(device, stream), device->cur) != AC_SUCCESS)
+        return AC_FAILURE;
     return copy_field_range(stream_of(device, stream), L,
                             device->blk[device->cur] + h * L.fstride, didx,
                             host_mesh.vertex_buffer[h] + sidx, (size_t)num_vertices, true, lo);
@@ -1046,14 +1079,19 @@ acDeviceStoreMesh(const Device device, const Stream stream, AcMesh* host_mesh)
 
 // device-to-device flat-range copy between two padded layouts
 __global__ void
-transfer_kernel(const Layout Ls, const state_t* __restrict__ src, long long s0, const Layout Ld,
-                state_t* __restrict__ dst, long long d0, long long count)
+transfer_kernel(const Layout Ls, const state_t* __restrict__ src, const float* __restrict__ slo,
+                long long s0, const Layout Ld, state_t* __restrict__ dst, float* __restrict__ dlo,
+                long long d0, long long count)
 {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
          t += (long long)gridDim.x * blockDim.x) {
         const long long a = s0 + t, b = d0 + t;
         const long long ra = a / Ls.mx, rb = b / Ld.mx;
-        dst[Ld.offx + rb * Ld.mxp + (b - rb * Ld.mx)] = src[Ls.offx + ra * Ls.mxp + (a - ra * Ls.mx)];
+        const long long ia = Ls.offx + ra * Ls.mxp + (a - ra * Ls.mx);
+        const long long ib = Ld.offx + rb * Ld.mxp + (b - rb * Ld.mx);
+        dst[ib]            = src[ia];
+        if (ACB_MIXED && dlo)
+            dlo[ib] = slo ? slo[ia] : 0.f; // the (hi, lo) pair moves whole
     }
 }
 
@@ -1076,10 +1114,20 @@ acDeviceTransferVertexBufferWithOffset(const Device src_device, const Stream str
     }
     cudaSetDevice(src_device->id);
     dst_device->ghost_ok[dst_device->cur] = false;
-    transfer_kernel<<<src_device->num_sms * 4, 256, 0, stream_of(src_device, stream)>>>(
-        src_device->L, src_device->blk[src_device->cur] + h * src_device->L.fstride,
+    const cudaStream_t tst = stream_of(src_device, stream);
+    if (ensure_lo_ghosts(src_device, tst, src_device->cur) != AC_SUCCESS ||
+        ensure_lo_ghosts(dst_device, tst, dst_device->cur) != AC_SUCCESS)
+        return AC_FAILURE;
+    const float* slo = src_device->lo[src_device->cur]
+                           ? src_device->lo[src_device->cur] + h * src_device->L.fstride
+                           : nullptr;
+    float* dlo = dst_device->lo[dst_device->cur]
+                     ? dst_device->lo[dst_device->cur] + h * dst_device->L.fstride
+                     : nullptr;
+    transfer_kernel<<<src_device->num_sms * 4, 256, 0, tst>>>(
+        src_device->L, src_device->blk[src_device->cur] + h * src_device->L.fstride, slo,
         (long long)sidx, dst_device->L, dst_device->blk[dst_device->cur] + h * dst_device->L.fstride,
-        (long long)didx, (long long)num_vertices);
+        dlo, (long long)didx, (long long)num_vertices);
     ACB_CUDA_CHECK(cudaGetLastError());
     src_device->launches++;
     return AC_SUCCESS;
@@ -1176,6 +1224,8 @@ acDeviceGeneralBoundcondStep(const Device device, const Stream stream,
     e.z = std::min(e.z, L.mz);
     if (e.x <= s.x || e.y <= s.y || e.z <= s.z)
         return AC_SUCCESS;
+    if (ensure_lo_ghosts(device, stream_of(device, stream), device->cur) != AC_SUCCESS)
+        return AC_FAILURE;
     HaloArgs a;
     a.L     = L;
     a.block = device->blk[device->cur];
@@ -1444,6 +1494,8 @@ acDeviceIntegrateSteps(const Device device, const Stream stream, const AcReal dt
             device->graph_launches[p] = device->launches - before;
             device->graph_ghost[p][0] = device->ghost_ok[0];
             device->graph_ghost[p][1] = device->ghost_ok[1];
+            device->graph_lo[p][0]    = device->lo_stale[0];
+            device->graph_lo[p][1]    = device->lo_stale[1];
             device->launches          = before;
             if (rc != AC_SUCCESS) {
                 cudaGraphDestroy(g);
@@ -1457,6 +1509,8 @@ acDeviceIntegrateSteps(const Device device, const Stream stream, const AcReal dt
         device->launches += device->graph_launches[p];
         device->ghost_ok[0] = device->graph_ghost[p][0]; // as the captured step left them
         device->ghost_ok[1] = device->graph_ghost[p][1];
+        device->lo_stale[0] = device->graph_lo[p][0];
+        device->lo_stale[1] = device->graph_lo[p][1];
         device->cur ^= 1; // three swaps per step
     }
     return AC_SUCCESS;

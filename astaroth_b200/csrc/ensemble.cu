@@ -196,7 +196,7 @@ build_tables(Ensemble e)
             d.P           = make_params(mb.uniforms, L, 0, 0);
             H[pos].L          = L;
             H[pos].block      = mb.blk[p];
-            H[pos].lo         = mb.lo[p];
+            H[pos].lo         = nullptr; // lo parts of ghosts: never read in an ensemble
             H[pos].unit_begin = units;
             H[pos].units_a    = (unsigned)halo_units_a(L);
             units += halo_units(L);

@@ -19,6 +19,9 @@
 //      thread has 4 (8) loads in flight.
 // A thread never stores before all its loads are issued, so memory-level
 // parallelism comes from the thread count, not from the warp count per row.
+// `lo` may be null: the mixed build's integration path fills the hi parts
+// only (the stencils never read the lo parts of ghosts), and fills the lo
+// parts on their own (as a block of floats) only when they are read.
 //
 // Sub-box fill (any start/end, any field range): one warp per (j, k) row of the
 // box, lane-strided; kept for the reference's partial-box API calls.
@@ -150,16 +153,16 @@ halo_unit(const Layout& L, state_t* block, float* lo, unsigned units_a, unsigned
                 float4* R       = reinterpret_cast<float4*>(F - L.offx);
                 const float4 vl = R[sl];
                 const float4 vr = R[sr];
-#if ACB_MIXED
-                float4* G       = reinterpret_cast<float4*>(lo + base - L.offx);
-                const float4 wl = G[sl];
-                const float4 wr = G[sr];
-#endif
                 R[gl] = vl;
                 R[gr] = vr;
 #if ACB_MIXED
-                G[gl] = wl;
-                G[gr] = wr;
+                if (lo) {
+                    float4* G       = reinterpret_cast<float4*>(lo + base - L.offx);
+                    const float4 wl = G[sl];
+                    const float4 wr = G[sr];
+                    G[gl]           = wl;
+                    G[gr]           = wr;
+                }
 #endif
                 return;
             }
@@ -170,24 +173,27 @@ halo_unit(const Layout& L, state_t* block, float* lo, unsigned units_a, unsigned
             v[q]          = F[L.nx + q]; // source of ghost q is nx + q
             v[NGHOST + q] = F[NGHOST + q]; // source of ghost nx + 3 + q is 3 + q
         }
-#if ACB_MIXED
-        float* G = lo + base;
-        float w[2 * NGHOST];
 #pragma unroll
         for (int q = 0; q < NGHOST; ++q) {
-            w[q]          = G[L.nx + q];
-            w[NGHOST + q] = G[NGHOST + q];
+            F[q]                 = v[q];
+            F[L.nx + NGHOST + q] = v[NGHOST + q];
         }
-#endif
-#pragma unroll
-        for (int q = 0; q < NGHOST; ++q) {
-            F[q]                   = v[q];
-            F[L.nx + NGHOST + q]   = v[NGHOST + q];
 #if ACB_MIXED
-            G[q]                   = w[q];
-            G[L.nx + NGHOST + q]   = w[NGHOST + q];
-#endif
+        if (lo) {
+            float* G = lo + base;
+            float w[2 * NGHOST];
+#pragma unroll
+            for (int q = 0; q < NGHOST; ++q) {
+                w[q]          = G[L.nx + q];
+                w[NGHOST + q] = G[NGHOST + q];
+            }
+#pragma unroll
+            for (int q = 0; q < NGHOST; ++q) {
+                G[q]                 = w[q];
+                G[L.nx + NGHOST + q] = w[NGHOST + q];
+            }
         }
+#endif
         return;
     }
     // kind B: 4 vertices, 32 apart, of a 128-vertex chunk of ghost row `row`
@@ -220,30 +226,35 @@ halo_unit(const Layout& L, state_t* block, float* lo, unsigned units_a, unsigned
     const long long s  = fo + lidx(L, 0, wrap_near(j, L.ny), wrap_near(k, L.nz));
     const int x0       = (int)(chunk * 128 + lane);
     state_t v[4];
-#if ACB_MIXED
-    float w[4];
-#endif
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int x = x0 + 32 * q;
-        if (x < L.mx) {
-            const int xs = wrap_near(x, L.nx);
-            v[q]         = block[s + xs];
-#if ACB_MIXED
-            w[q] = lo[s + xs];
-#endif
-        }
+        if (x < L.mx)
+            v[q] = block[s + wrap_near(x, L.nx)];
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int x = x0 + 32 * q;
-        if (x < L.mx) {
+        if (x < L.mx)
             block[d + x] = v[q];
+    }
 #if ACB_MIXED
-            lo[d + x] = w[q];
-#endif
+    if (lo) {
+        float w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int x = x0 + 32 * q;
+            if (x < L.mx)
+                w[q] = lo[s + wrap_near(x, L.nx)];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int x = x0 + 32 * q;
+            if (x < L.mx)
+                lo[d + x] = w[q];
         }
     }
+#endif
 }
 
 static __global__ void __launch_bounds__(256)

@@ -401,6 +401,31 @@ def test_reference_ctest_sample_runs(tmp_path):
     assert "FAIL" not in r.stdout
 
 
+@pytest.mark.parametrize("flavour", FLAVOURS)
+def test_transfer_moves_whole_values(flavour):
+    """acDeviceTransferMesh between two Devices on one GPU copies the whole
+    state: in the mixed build the (hi, lo) pairs, and after a whole-box ghost
+    fill (which writes only the hi parts on the integration path) the ghosts'
+    lo parts too; the double views of source and destination are identical."""
+    prec = abi.PRECISIONS[flavour]
+    n = 16
+    info = workload_info(prec, n)
+    fields = init.workload_fields(n, n, n, prec.np_dtype, seed=41, amplitude=0.05,
+                                  velocity_mode=0.1)
+    with new_device(flavour, info) as a, new_device(flavour, info) as b:
+        a.load_mesh(abi.HostMesh(prec, info, [f.copy() for f in fields]))
+        for _ in range(2):
+            a.integrate_step(1e-3)
+        a.periodic_boundconds()
+        assert a.lib.acDeviceTransferMesh(a.handle, 0, b.handle) == abi.AC_SUCCESS
+        a.synchronize()
+        src = [a.store_double(w) for w in range(8)]
+        dst = [b.store_double(w) for w in range(8)]
+    for w in range(8):
+        assert np.array_equal(src[w], dst[w]), w
+        assert np.array_equal(src[w], init.wrap_ghosts(interior(src[w]))), w
+
+
 def mirror_fill_numpy(a, sign):
     """Restatement of the symmetric/antisymmetric fill as the reference intends it
     (src/core/kernels/boundconds.cuh:3-128): each ghost vertex takes sign times
