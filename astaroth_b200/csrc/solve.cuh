@@ -528,9 +528,10 @@ push_queue(ZQueue<float>& Q, float f0, const float* dx, const float* dy)
     Q.v1 = f0;
 }
 
-// field_derivs_q of two fields at once: every pencil sum and difference, the
-// xy diagonals both fields need and the paired z diagonals in packed lanes;
-// the coefficient sums per field exactly as field_derivs_q forms them.
+// The derivatives of two fields at once (field_derivs_q's stencils): every
+// pencil sum and difference, the xy diagonals both fields need and the paired
+// z diagonals in packed lanes; the coefficient sums per field. Second
+// derivatives in difference form (below).
 template <int BX, class FA, class FB>
 __device__ __forceinline__ void
 pair_derivs_q(const float* __restrict__ cA, const float* __restrict__ cB, const int* zo,
@@ -538,33 +539,34 @@ pair_derivs_q(const float* __restrict__ cA, const float* __restrict__ cB, const 
               FieldDerivs<float>& rA, FieldDerivs<float>& rB)
 {
     const float a0 = cA[0], b0 = cB[0];
-    rA.v = a0;
-    rB.v = b0;
+    rA.v        = a0;
+    rB.v        = b0;
+    const F2 F0 = pk2(a0, b0);
     float dxA[3], dxB[3], sxA[3], sxB[3], dyA[3], dyB[3], syA[3], syB[3], dzA[3], dzB[3],
         szA[3], szB[3];
+    // Second differences as u + v with u = f(+k) - f0, v = f(-k) - f0: for a
+    // smooth field u and v are exact in FP32 (Sterbenz), so f(+k) + f(-k) - 2 f0
+    // keeps its digits instead of cancelling terms of size |c0 f0| (about
+    // 2.7 f / ds^2); mathematically the same stencil (c0 = -2 (c1 + c2 + c3)).
+    // First differences f(+k) - f(-k) directly, as prime_queue forms the queued
+    // ones, so results do not depend on where a task's z segment starts.
+    auto dsum = [&](F2 p, F2 m, float& dA, float& dB, float& sA, float& sB) {
+        upk2(sub2(p, m), dA, dB);
+        upk2(add2(sub2(p, F0), sub2(m, F0)), sA, sB);
+    };
 #pragma unroll
     for (int k = 1; k <= 3; ++k) {
-        const F2 px = pk2(cA[k], cB[k]), mx = pk2(cA[-k], cB[-k]);
-        upk2(sub2(px, mx), dxA[k - 1], dxB[k - 1]);
-        upk2(add2(px, mx), sxA[k - 1], sxB[k - 1]);
-        const F2 py = pk2(cA[k * BX], cB[k * BX]), my = pk2(cA[-k * BX], cB[-k * BX]);
-        upk2(sub2(py, my), dyA[k - 1], dyB[k - 1]);
-        upk2(add2(py, my), syA[k - 1], syB[k - 1]);
+        dsum(pk2(cA[k], cB[k]), pk2(cA[-k], cB[-k]), dxA[k - 1], dxB[k - 1], sxA[k - 1],
+             sxB[k - 1]);
+        dsum(pk2(cA[k * BX], cB[k * BX]), pk2(cA[-k * BX], cB[-k * BX]), dyA[k - 1], dyB[k - 1],
+             syA[k - 1], syB[k - 1]);
     }
-    {
-        const F2 p1 = pk2(cA[zo[4]], cB[zo[4]]), p2 = pk2(cA[zo[5]], cB[zo[5]]),
-                 p3 = pk2(cA[zo[6]], cB[zo[6]]);
-        const F2 m1 = pk2(QA.v1, QB.v1), m2 = pk2(QA.v2, QB.v2), m3 = pk2(QA.v3, QB.v3);
-        upk2(sub2(p1, m1), dzA[0], dzB[0]);
-        upk2(sub2(p2, m2), dzA[1], dzB[1]);
-        upk2(sub2(p3, m3), dzA[2], dzB[2]);
-        upk2(add2(p1, m1), szA[0], szB[0]);
-        upk2(add2(p2, m2), szA[1], szB[1]);
-        upk2(add2(p3, m3), szA[2], szB[2]);
-    }
+    dsum(pk2(cA[zo[4]], cB[zo[4]]), pk2(QA.v1, QB.v1), dzA[0], dzB[0], szA[0], szB[0]);
+    dsum(pk2(cA[zo[5]], cB[zo[5]]), pk2(QA.v2, QB.v2), dzA[1], dzB[1], szA[1], szB[1]);
+    dsum(pk2(cA[zo[6]], cB[zo[6]]), pk2(QA.v3, QB.v3), dzA[2], dzB[2], szA[2], szB[2]);
     auto first = [&](const float* c1, const float* d) { return c1[0] * d[0] + c1[1] * d[1] + c1[2] * d[2]; };
-    auto second = [&](const float* c2, float f0, const float* s) {
-        return c2[0] * f0 + c2[1] * s[0] + c2[2] * s[1] + c2[3] * s[2];
+    auto second = [&](const float* c2, float, const float* s) {
+        return c2[1] * s[0] + c2[2] * s[1] + c2[3] * s[2];
     };
     if (FA::GX) rA.gx = first(P.c1[0], dxA);
     if (FB::GX) rB.gx = first(P.c1[0], dxB);
