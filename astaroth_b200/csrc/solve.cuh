@@ -1024,22 +1024,9 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
                     load_centre<STEP>(L, out, in_lo, out_lo, id + L.plane, cv_next);
             }
             else if constexpr (CT) {
-                // from the centre slot the producer filled by TMA
-                const float* cs = centre + (size_t)(oq % Cfg::NC) * (Cfg::centre_slot_bytes() / 4) +
-                                  ty * TX + tx;
-                constexpr int FS = Cfg::TX * Cfg::TY;
-#pragma unroll
-                for (int f = 0; f < ACB_NF; ++f) {
-                    if constexpr (CS::PREV)
-                        cv.prev[f] = cs[CS::POS_PREV * Cfg::CENTRE + f * FS];
-#if ACB_MIXED
-                    cv.cur_lo[f] = cs[CS::POS_CUR_LO * Cfg::CENTRE + f * FS];
-                    if constexpr (CS::PREV)
-                        cv.prev_lo[f] = cs[CS::POS_PREV_LO * Cfg::CENTRE + f * FS];
-                    else
-                        cv.prev_lo[f] = 0.f;
-#endif
-                }
+                // read from the centre slot after the right-hand sides (below):
+                // the values are in shared memory already, and reading them
+                // late keeps 24 registers free through the stencils
             }
             else {
                 load_centre<STEP>(L, out, in_lo, out_lo, id, cv);
@@ -1064,6 +1051,25 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
             T fo[3] = {0, 0, 0};
             if constexpr (STEP == 3)
                 acb::forcing_at<T>(a.P, i, j, k, fo);
+
+            if constexpr (CT) {
+                // from the centre slot the producer filled by TMA
+                const float* cs = centre + (size_t)(oq % Cfg::NC) * (Cfg::centre_slot_bytes() / 4) +
+                                  ty * TX + tx;
+                constexpr int FS = Cfg::TX * Cfg::TY;
+#pragma unroll
+                for (int f = 0; f < ACB_NF; ++f) {
+                    if constexpr (CS::PREV)
+                        cv.prev[f] = cs[CS::POS_PREV * Cfg::CENTRE + f * FS];
+#if ACB_MIXED
+                    cv.cur_lo[f] = cs[CS::POS_CUR_LO * Cfg::CENTRE + f * FS];
+                    if constexpr (CS::PREV)
+                        cv.prev_lo[f] = cs[CS::POS_PREV_LO * Cfg::CENTRE + f * FS];
+                    else
+                        cv.prev_lo[f] = 0.f;
+#endif
+                }
+            }
 
 #pragma unroll
             for (int f = 0; f < ACB_NF; ++f) {
