@@ -270,132 +270,79 @@ field_derivs(const state_t* __restrict__ c, const int* zo, const SolveParams<T>&
 
 // Register queue of one field along z (2.5D streaming): the values of the
 // thread's own column at the three planes below the current one, and, for a
-// field with an xz (yz) cross derivative, the x (y) differences
-// d_k = f(+k) - f(-k) of those planes. The diagonal cross derivative
+// field with an xz (yz) cross derivative, the lower half of that derivative
+// as running sums. The diagonal cross derivative at plane z,
 //   sum_k e_k (f(+k,+k) + f(-k,-k) - f(+k,-k) - f(-k,+k))
-// equals sum_k e_k (d_k(z+k) - d_k(z-k)), so its lower half comes from the
-// queue and only the upper half is read from the ring; likewise the lower
-// half of the z pencil.
+//     = U(z) - L(z),  U(z) = sum_k e_k d_k(z+k),  L(z) = sum_k e_k d_k(z-k),
+// with d_k(w) = f(+k) - f(-k) the x (y) difference at plane w: the differences
+// of the current plane are formed for the first derivative anyway, and each
+// contributes e_k d_k(z) to L(z+k). So the queue keeps
+//   a1 = L(z),  a2 = the part of L(z+1) known so far,  a3 = that of L(z+2),
+// and advancing a plane is three fused multiply-adds (no register moves):
+//   a1 <- e1 d1(z) + a2,  a2 <- e2 d2(z) + a3,  a3 <- e3 d3(z).
+// Only the upper half U is read from the ring.
 template <typename T>
 struct ZQueue {
-    T v1, v2, v3;                  // f at z-1, z-2, z-3
-    T x1, x2a, x2b, x3a, x3b, x3c; // dx_1(z-1); dx_2(z-1), dx_2(z-2); dx_3(z-1), (z-2), (z-3)
-    T y1, y2a, y2b, y3a, y3b, y3c; // the same for dy
+    T v1, v2, v3;    // f at z-1, z-2, z-3
+    T xa1, xa2, xa3; // xz lower half: L(z), partial L(z+1), partial L(z+2)
+    T ya1, ya2, ya3; // the same for yz
 };
+
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+
+// Advances the lower-half sums of one z diagonal past the plane whose
+// differences are d1, d2, d3 (e: the diagonal's coefficients). The rounding
+// sequence is fixed (explicit fma / mul), so prime_queue below reproduces the
+// sums a streaming task would have built, bit for bit.
+__device__ __forceinline__ void
+zacc_push(float& a1, float& a2, float& a3, const float* e, float d1, float d2, float d3)
+{
+    a1 = fma_rn(e[0], d1, a2);
+    a2 = fma_rn(e[1], d2, a3);
+    a3 = mul_rn(e[2], d3);
+}
+
+// Lower-half sums of one z diagonal at the first plane of a task from the
+// three planes below it (zo[0..2]); step: 1 for xz, the row pitch for yz.
+__device__ __forceinline__ void
+zacc_prime(const float* __restrict__ c, const int* zo, int step, const float* e, float& a1,
+           float& a2, float& a3)
+{
+    auto d = [&](int plane, int k) { return c[zo[plane] + k * step] - c[zo[plane] - k * step]; };
+    // plane z-3: only its third difference reaches L(z)
+    const float t3 = mul_rn(e[2], d(0, 3));
+    // plane z-2
+    const float b2 = fma_rn(e[1], d(1, 2), t3);
+    const float b3 = mul_rn(e[2], d(1, 3));
+    // plane z-1
+    a1 = fma_rn(e[0], d(2, 1), b2);
+    a2 = fma_rn(e[1], d(2, 2), b3);
+    a3 = mul_rn(e[2], d(2, 3));
+}
+
+// Upper half U of one z diagonal (u1..u3: d_k at plane z+k), in the order
+// every caller uses.
+__device__ __forceinline__ float
+zacc_upper(const float* e, float u1, float u2, float u3)
+{
+    return fma_rn(e[2], u3, fma_rn(e[1], u2, mul_rn(e[0], u1)));
+}
 
 // Fills the queue from the ring at the first plane of a task (zo[0..2]: the
 // three planes below it).
-template <typename T, int BX, bool XZ, bool YZ>
+template <int BX, bool XZ, bool YZ>
 __device__ __forceinline__ void
-prime_queue(const state_t* __restrict__ c, const int* zo, ZQueue<T>& Q)
+prime_queue(const float* __restrict__ c, const int* zo, const SolveParams<float>& P,
+            ZQueue<float>& Q)
 {
     Q.v1 = c[zo[2]];
     Q.v2 = c[zo[1]];
     Q.v3 = c[zo[0]];
-    if (XZ) {
-        Q.x1  = (T)c[zo[2] + 1] - (T)c[zo[2] - 1];
-        Q.x2a = (T)c[zo[2] + 2] - (T)c[zo[2] - 2];
-        Q.x2b = (T)c[zo[1] + 2] - (T)c[zo[1] - 2];
-        Q.x3a = (T)c[zo[2] + 3] - (T)c[zo[2] - 3];
-        Q.x3b = (T)c[zo[1] + 3] - (T)c[zo[1] - 3];
-        Q.x3c = (T)c[zo[0] + 3] - (T)c[zo[0] - 3];
-    }
-    if (YZ) {
-        Q.y1  = (T)c[zo[2] + BX] - (T)c[zo[2] - BX];
-        Q.y2a = (T)c[zo[2] + 2 * BX] - (T)c[zo[2] - 2 * BX];
-        Q.y2b = (T)c[zo[1] + 2 * BX] - (T)c[zo[1] - 2 * BX];
-        Q.y3a = (T)c[zo[2] + 3 * BX] - (T)c[zo[2] - 3 * BX];
-        Q.y3b = (T)c[zo[1] + 3 * BX] - (T)c[zo[1] - 3 * BX];
-        Q.y3c = (T)c[zo[0] + 3 * BX] - (T)c[zo[0] - 3 * BX];
-    }
-}
-
-// field_derivs with the lower z half from the queue; advances the queue by one
-// plane. Ring reads: x and y pencils (12), centre (1), upper z half (3), upper
-// halves of the xz / yz diagonals (6 each) and the whole xy diagonal (12),
-// i.e. 16 + 6 * (XZ + YZ) + 12 * XY instead of 19 + 12 * (XY + XZ + YZ).
-template <typename T, int BX, bool GX, bool GY, bool GZ, bool XY, bool XZ, bool YZ>
-__device__ __forceinline__ FieldDerivs<T>
-field_derivs_q(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, ZQueue<T>& Q)
-{
-    FieldDerivs<T> r;
-    const T f0 = (T)c[0];
-    r.v        = f0;
-    T dx1, dx2, dx3, dy1, dy2, dy3;
-    // x pencil
-    {
-        const T m1 = c[-1], p1 = c[1], m2 = c[-2], p2 = c[2], m3 = c[-3], p3 = c[3];
-        dx1 = p1 - m1;
-        dx2 = p2 - m2;
-        dx3 = p3 - m3;
-        if (GX)
-            r.gx = P.c1[0][0] * dx1 + P.c1[0][1] * dx2 + P.c1[0][2] * dx3;
-        r.xx = dd2(f0, m1, p1, m2, p2, m3, p3, P.c2[0]);
-    }
-    // y pencil
-    {
-        const T m1 = c[-BX], p1 = c[BX], m2 = c[-2 * BX], p2 = c[2 * BX], m3 = c[-3 * BX],
-                p3 = c[3 * BX];
-        dy1 = p1 - m1;
-        dy2 = p2 - m2;
-        dy3 = p3 - m3;
-        if (GY)
-            r.gy = P.c1[1][0] * dy1 + P.c1[1][1] * dy2 + P.c1[1][2] * dy3;
-        r.yy = dd2(f0, m1, p1, m2, p2, m3, p3, P.c2[1]);
-    }
-    // z pencil: lower half from the queue
-    {
-        const T m1 = Q.v1, m2 = Q.v2, m3 = Q.v3;
-        const T p1 = c[zo[4]], p2 = c[zo[5]], p3 = c[zo[6]];
-        if (GZ)
-            d12(f0, m1, p1, m2, p2, m3, p3, P.c1[2], P.c2[2], r.gz, r.zz);
-        else
-            r.zz = dd2(f0, m1, p1, m2, p2, m3, p3, P.c2[2]);
-    }
-    if (XY) {
-        T s = 0;
-#pragma unroll
-        for (int k = 1; k <= 3; ++k) {
-            const T a = (T)c[k + k * BX] + (T)c[-k - k * BX];
-            const T b = (T)c[k - k * BX] + (T)c[-k + k * BX];
-            s += P.cx[0][k - 1] * (a - b);
-        }
-        r.xy = s;
-    }
-    if (XZ) {
-        const T u1 = (T)c[zo[4] + 1] - (T)c[zo[4] - 1];
-        const T u2 = (T)c[zo[5] + 2] - (T)c[zo[5] - 2];
-        const T u3 = (T)c[zo[6] + 3] - (T)c[zo[6] - 3];
-        T s = P.cx[1][0] * (u1 - Q.x1);
-        s += P.cx[1][1] * (u2 - Q.x2b);
-        s += P.cx[1][2] * (u3 - Q.x3c);
-        r.xz  = s;
-        Q.x3c = Q.x3b;
-        Q.x3b = Q.x3a;
-        Q.x3a = dx3;
-        Q.x2b = Q.x2a;
-        Q.x2a = dx2;
-        Q.x1  = dx1;
-    }
-    if (YZ) {
-        const T u1 = (T)c[zo[4] + BX] - (T)c[zo[4] - BX];
-        const T u2 = (T)c[zo[5] + 2 * BX] - (T)c[zo[5] - 2 * BX];
-        const T u3 = (T)c[zo[6] + 3 * BX] - (T)c[zo[6] - 3 * BX];
-        T s = P.cx[2][0] * (u1 - Q.y1);
-        s += P.cx[2][1] * (u2 - Q.y2b);
-        s += P.cx[2][2] * (u3 - Q.y3c);
-        r.yz  = s;
-        Q.y3c = Q.y3b;
-        Q.y3b = Q.y3a;
-        Q.y3a = dy3;
-        Q.y2b = Q.y2a;
-        Q.y2a = dy2;
-        Q.y1  = dy1;
-    }
-    Q.v3 = Q.v2;
-    Q.v2 = Q.v1;
-    Q.v1 = f0;
-    return r;
+    if (XZ)
+        zacc_prime(c, zo, 1, P.cx[1], Q.xa1, Q.xa2, Q.xa3);
+    if (YZ)
+        zacc_prime(c, zo, BX, P.cx[2], Q.ya1, Q.ya2, Q.ya3);
 }
 
 // ---- pairs of fields in packed FP32 lanes ----------------------------------
@@ -442,20 +389,20 @@ struct DFlags {
     static constexpr bool GX = GX_, GY = GY_, GZ = GZ_, XY = XY_, XZ = XZ_, YZ = YZ_;
 };
 
-// Upper half of a z-diagonal cross derivative (XK: xz, else yz) of one lane:
-// the ring offsets of its two points at plane z+k and its queued lower half.
+// A z-diagonal cross derivative (XK: xz, else yz) of one lane: the ring step
+// of its points, its coefficients and its queued lower half.
 template <bool XK, int BX>
 struct ZCross {
     static constexpr int step = XK ? 1 : BX;
-    __device__ __forceinline__ static float past(const ZQueue<float>& Q, int k)
+    static constexpr int row  = XK ? 1 : 2;
+    __device__ __forceinline__ static float lower(const ZQueue<float>& Q)
     {
-        return XK ? (k == 1 ? Q.x1 : (k == 2 ? Q.x2b : Q.x3c))
-                  : (k == 1 ? Q.y1 : (k == 2 ? Q.y2b : Q.y3c));
+        return XK ? Q.xa1 : Q.ya1;
     }
 };
 
 // Two z-diagonal cross derivatives (one of field A, kind XA; one of field B,
-// kind XB) with their differences formed in packed lanes.
+// kind XB) with the upper-half differences formed in packed lanes.
 template <bool XA, bool XB, int BX>
 __device__ __forceinline__ void
 zcross_pair(const float* __restrict__ cA, const float* __restrict__ cB, const int* zo,
@@ -467,21 +414,13 @@ zcross_pair(const float* __restrict__ cA, const float* __restrict__ cB, const in
     float a[3], b[3];
 #pragma unroll
     for (int k = 1; k <= 3; ++k) {
-        const int z  = zo[3 + k];
-        const F2 u   = sub2(pk2(cA[z + k * CA::step], cB[z + k * CB::step]),
-                            pk2(cA[z - k * CA::step], cB[z - k * CB::step]));
-        const F2 w   = sub2(u, pk2(CA::past(QA, k), CB::past(QB, k)));
-        upk2(w, a[k - 1], b[k - 1]);
+        const int z = zo[3 + k];
+        const F2 u  = sub2(pk2(cA[z + k * CA::step], cB[z + k * CB::step]),
+                           pk2(cA[z - k * CA::step], cB[z - k * CB::step]));
+        upk2(u, a[k - 1], b[k - 1]);
     }
-    const int ra = XA ? 1 : 2, rb = XB ? 1 : 2;
-    float s = P.cx[ra][0] * a[0];
-    s += P.cx[ra][1] * a[1];
-    s += P.cx[ra][2] * a[2];
-    sA = s;
-    float t = P.cx[rb][0] * b[0];
-    t += P.cx[rb][1] * b[1];
-    t += P.cx[rb][2] * b[2];
-    sB = t;
+    sA = zacc_upper(P.cx[CA::row], a[0], a[1], a[2]) - CA::lower(QA);
+    sB = zacc_upper(P.cx[CB::row], b[0], b[1], b[2]) - CB::lower(QB);
 }
 
 // One z-diagonal cross derivative of one field (no partner).
@@ -491,44 +430,32 @@ zcross_one(const float* __restrict__ c, const int* zo, const SolveParams<float>&
            const ZQueue<float>& Q)
 {
     using CK = ZCross<XK, BX>;
-    const int r = XK ? 1 : 2;
-    float s     = 0;
+    float u[3];
 #pragma unroll
     for (int k = 1; k <= 3; ++k) {
-        const int z   = zo[3 + k];
-        const float u = c[z + k * CK::step] - c[z - k * CK::step];
-        s += P.cx[r][k - 1] * (u - CK::past(Q, k));
+        const int z = zo[3 + k];
+        u[k - 1]    = c[z + k * CK::step] - c[z - k * CK::step];
     }
-    return s;
+    return zacc_upper(P.cx[CK::row], u[0], u[1], u[2]) - CK::lower(Q);
 }
 
-// Advances a single-precision queue by one plane (after every use of it).
+// Advances a queue by one plane (after every use of it): f0 and the x / y
+// differences dx, dy of the plane just done.
 template <bool XZ, bool YZ>
 __device__ __forceinline__ void
-push_queue(ZQueue<float>& Q, float f0, const float* dx, const float* dy)
+push_queue(ZQueue<float>& Q, const SolveParams<float>& P, float f0, const float* dx,
+           const float* dy)
 {
-    if (XZ) {
-        Q.x3c = Q.x3b;
-        Q.x3b = Q.x3a;
-        Q.x3a = dx[2];
-        Q.x2b = Q.x2a;
-        Q.x2a = dx[1];
-        Q.x1  = dx[0];
-    }
-    if (YZ) {
-        Q.y3c = Q.y3b;
-        Q.y3b = Q.y3a;
-        Q.y3a = dy[2];
-        Q.y2b = Q.y2a;
-        Q.y2a = dy[1];
-        Q.y1  = dy[0];
-    }
+    if (XZ)
+        zacc_push(Q.xa1, Q.xa2, Q.xa3, P.cx[1], dx[0], dx[1], dx[2]);
+    if (YZ)
+        zacc_push(Q.ya1, Q.ya2, Q.ya3, P.cx[2], dy[0], dy[1], dy[2]);
     Q.v3 = Q.v2;
     Q.v2 = Q.v1;
     Q.v1 = f0;
 }
 
-// The derivatives of two fields at once (field_derivs_q's stencils): every
+// The derivatives of two fields at once: every
 // pencil sum and difference, the xy diagonals both fields need and the paired
 // z diagonals in packed lanes; the coefficient sums per field. Second
 // derivatives in difference form (below).
@@ -637,8 +564,8 @@ pair_derivs_q(const float* __restrict__ cA, const float* __restrict__ cB, const 
     if (FB::XZ) rB.xz = zB[0];
     if (FB::YZ) rB.yz = FB::XZ ? zB[1] : zB[0];
 
-    push_queue<FA::XZ, FA::YZ>(QA, a0, dxA, dyA);
-    push_queue<FB::XZ, FB::YZ>(QB, b0, dxB, dyB);
+    push_queue<FA::XZ, FA::YZ>(QA, P, a0, dxA, dyA);
+    push_queue<FB::XZ, FB::YZ>(QB, P, b0, dxB, dyB);
 }
 
 // Derivative flags of the eight fields: what the right-hand sides use.
@@ -677,50 +604,38 @@ mhd_rhs(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, T
     rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
 }
 
-// The same with the z register queues.
-template <typename T, int BX, int FIELD>
+// The same with the z register queues (single-precision stencils), in pairs
+// of like-shaped stencils, two packed lanes per instruction.
+template <int BX, int FIELD>
 __device__ __forceinline__ void
-mhd_rhs_q(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, T roc[ACB_NF],
-          T cur[ACB_NF], ZQueue<T> (&Q)[ACB_NF])
+mhd_rhs_q(const float* __restrict__ c, const int* zo, const SolveParams<float>& P,
+          float roc[ACB_NF], float cur[ACB_NF], ZQueue<float> (&Q)[ACB_NF])
 {
-    if constexpr (sizeof(T) == 4 && sizeof(state_t) == 4) {
-        // in pairs of like-shaped stencils, two packed lanes per instruction
-        FieldDerivs<T> lr, ux, uy, uz, ax, ay, az, ss;
-        pair_derivs_q<BX, DFlags<ACB_D_LNRHO>, DFlags<ACB_D_SS>>(c + 0 * FIELD, c + 7 * FIELD, zo,
-                                                                 P, Q[0], Q[7], lr, ss);
-        pair_derivs_q<BX, DFlags<ACB_D_UUX>, DFlags<ACB_D_UUY>>(c + 1 * FIELD, c + 2 * FIELD, zo,
-                                                                P, Q[1], Q[2], ux, uy);
-        pair_derivs_q<BX, DFlags<ACB_D_AX>, DFlags<ACB_D_AY>>(c + 4 * FIELD, c + 5 * FIELD, zo, P,
-                                                              Q[4], Q[5], ax, ay);
-        pair_derivs_q<BX, DFlags<ACB_D_UUZ>, DFlags<ACB_D_AZ>>(c + 3 * FIELD, c + 6 * FIELD, zo,
-                                                               P, Q[3], Q[6], uz, az);
-        rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
-    }
-    else {
-        const auto lr = field_derivs_q<T, BX, ACB_D_LNRHO>(c + 0 * FIELD, zo, P, Q[0]);
-        const auto ux = field_derivs_q<T, BX, ACB_D_UUX>(c + 1 * FIELD, zo, P, Q[1]);
-        const auto uy = field_derivs_q<T, BX, ACB_D_UUY>(c + 2 * FIELD, zo, P, Q[2]);
-        const auto uz = field_derivs_q<T, BX, ACB_D_UUZ>(c + 3 * FIELD, zo, P, Q[3]);
-        const auto ax = field_derivs_q<T, BX, ACB_D_AX>(c + 4 * FIELD, zo, P, Q[4]);
-        const auto ay = field_derivs_q<T, BX, ACB_D_AY>(c + 5 * FIELD, zo, P, Q[5]);
-        const auto az = field_derivs_q<T, BX, ACB_D_AZ>(c + 6 * FIELD, zo, P, Q[6]);
-        const auto ss = field_derivs_q<T, BX, ACB_D_SS>(c + 7 * FIELD, zo, P, Q[7]);
-        rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
-    }
+    FieldDerivs<float> lr, ux, uy, uz, ax, ay, az, ss;
+    pair_derivs_q<BX, DFlags<ACB_D_LNRHO>, DFlags<ACB_D_SS>>(c + 0 * FIELD, c + 7 * FIELD, zo, P,
+                                                             Q[0], Q[7], lr, ss);
+    pair_derivs_q<BX, DFlags<ACB_D_UUX>, DFlags<ACB_D_UUY>>(c + 1 * FIELD, c + 2 * FIELD, zo, P,
+                                                            Q[1], Q[2], ux, uy);
+    pair_derivs_q<BX, DFlags<ACB_D_AX>, DFlags<ACB_D_AY>>(c + 4 * FIELD, c + 5 * FIELD, zo, P,
+                                                          Q[4], Q[5], ax, ay);
+    pair_derivs_q<BX, DFlags<ACB_D_UUZ>, DFlags<ACB_D_AZ>>(c + 3 * FIELD, c + 6 * FIELD, zo, P,
+                                                           Q[3], Q[6], uz, az);
+    rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
 }
 
-template <typename T, int BX, int FIELD>
+template <int BX, int FIELD>
 __device__ __forceinline__ void
-prime_queues(const state_t* __restrict__ c, const int* zo, ZQueue<T> (&Q)[ACB_NF])
+prime_queues(const float* __restrict__ c, const int* zo, const SolveParams<float>& P,
+             ZQueue<float> (&Q)[ACB_NF])
 {
-    prime_queue<T, BX, false, false>(c + 0 * FIELD, zo, Q[0]);
-    prime_queue<T, BX, true, false>(c + 1 * FIELD, zo, Q[1]);
-    prime_queue<T, BX, false, true>(c + 2 * FIELD, zo, Q[2]);
-    prime_queue<T, BX, true, true>(c + 3 * FIELD, zo, Q[3]);
-    prime_queue<T, BX, true, false>(c + 4 * FIELD, zo, Q[4]);
-    prime_queue<T, BX, false, true>(c + 5 * FIELD, zo, Q[5]);
-    prime_queue<T, BX, true, true>(c + 6 * FIELD, zo, Q[6]);
-    prime_queue<T, BX, false, false>(c + 7 * FIELD, zo, Q[7]);
+    prime_queue<BX, false, false>(c + 0 * FIELD, zo, P, Q[0]);
+    prime_queue<BX, true, false>(c + 1 * FIELD, zo, P, Q[1]);
+    prime_queue<BX, false, true>(c + 2 * FIELD, zo, P, Q[2]);
+    prime_queue<BX, true, true>(c + 3 * FIELD, zo, P, Q[3]);
+    prime_queue<BX, true, false>(c + 4 * FIELD, zo, P, Q[4]);
+    prime_queue<BX, false, true>(c + 5 * FIELD, zo, P, Q[5]);
+    prime_queue<BX, true, true>(c + 6 * FIELD, zo, P, Q[6]);
+    prime_queue<BX, false, false>(c + 7 * FIELD, zo, P, Q[7]);
 }
 
 // Right-hand sides from the derivative sets (stencil_kernel.ac:355-528,
@@ -968,7 +883,7 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
     // precision has no registers to spare for them and reads every operand
     // from the ring
     constexpr bool QZ = sizeof(state_t) == 4;
-    acb::ZQueue<T> Q[ACB_NF];
+    acb::ZQueue<float> Q[ACB_NF];
     if constexpr (QZ) {
         if (ok && act) {
             const uint32_t sc = (q + NGHOST) % NP;
@@ -977,7 +892,7 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
             for (int dz = -NGHOST; dz <= NGHOST; ++dz)
                 zo[dz + NGHOST] = ((int)((q + NGHOST + dz) % NP) - (int)sc) * PLANE;
             const state_t* c = ring + (size_t)sc * PLANE + (ty + NGHOST) * BX + (tx + 4);
-            acb::prime_queues<T, BX, FIELD>(c, zo, Q);
+            acb::prime_queues<BX, FIELD>(c, zo, P, Q);
         }
         // the three planes below the first output plane now live in the queues
         __syncwarp();
@@ -1044,7 +959,7 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
 
             T roc[ACB_NF], cur[ACB_NF];
             if constexpr (QZ)
-                acb::mhd_rhs_q<T, BX, FIELD>(c, zo, P, roc, cur, Q);
+                acb::mhd_rhs_q<BX, FIELD>(c, zo, P, roc, cur, Q);
             else
                 acb::mhd_rhs<T, BX, FIELD>(c, zo, P, roc, cur);
 
