@@ -779,6 +779,34 @@ pair_add(float hi, float lo, float d, float& ohi, float& olo)
     olo            = l - (ohi - s);
 }
 
+__device__ __forceinline__ F2
+mul2(F2 a, F2 b)
+{
+    F2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+
+__device__ __forceinline__ F2
+fma2(F2 a, F2 b, F2 c)
+{
+    F2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return r;
+}
+
+// pair_add of two fields in packed lanes (the same operations lane by lane).
+__device__ __forceinline__ void
+pair_add2(F2 hi, F2 lo, F2 d, F2& ohi, F2& olo)
+{
+    const F2 s  = add2(hi, d);
+    const F2 bb = sub2(s, hi);
+    const F2 e  = add2(sub2(hi, sub2(s, bb)), sub2(d, bb));
+    const F2 l  = add2(lo, e);
+    ohi         = add2(s, l);
+    olo         = sub2(l, sub2(ohi, s));
+}
+
 } // namespace acb
 
 // Values of the vertex's own column that the update needs besides the ring:
@@ -986,19 +1014,48 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
                 }
             }
 
+#if ACB_MIXED
+            // The compensated update, two fields per instruction in the field
+            // pairs of the stencils (packed lanes; per lane the operations and
+            // rounding of pair_add):
+            //   d = rkB * roc (+ rkA * ((cur - prev) + (cur_lo - prev_lo)))
+            //   (hi, lo) = (cur, cur_lo) + d  [+ forcing of ux, uy, uz]
+            {
+                constexpr int FA[4] = {0, 1, 4, 3}, FB[4] = {7, 2, 5, 6};
+                const acb::F2 rkA2 = acb::pk2(rkA, rkA), rkB2 = acb::pk2(rkB, rkB);
+#pragma unroll
+                for (int pr = 0; pr < 4; ++pr) {
+                    const int fa = FA[pr], fb = FB[pr];
+                    const acb::F2 c2 = acb::pk2(cur[fa], cur[fb]);
+                    const acb::F2 l2 = acb::pk2(cv.cur_lo[fa], cv.cur_lo[fb]);
+                    acb::F2 d2       = acb::mul2(rkB2, acb::pk2(roc[fa], roc[fb]));
+                    if (STEP > 0) {
+                        const acb::F2 x =
+                            acb::add2(acb::sub2(c2, acb::pk2(cv.prev[fa], cv.prev[fb])),
+                                      acb::sub2(l2, acb::pk2(cv.prev_lo[fa], cv.prev_lo[fb])));
+                        d2 = acb::fma2(rkA2, x, d2);
+                    }
+                    acb::F2 h2, o2;
+                    acb::pair_add2(c2, l2, d2, h2, o2);
+                    if (STEP == 3 && (pr == 1 || pr == 3)) {
+                        // ux, uy; uz with az, whose lane adds 0 (a pair that
+                        // pair_add returned is left as it is by adding 0)
+                        const acb::F2 f2 =
+                            pr == 1 ? acb::pk2(fo[0], fo[1]) : acb::pk2(fo[2], 0.f);
+                        acb::pair_add2(h2, o2, f2, h2, o2);
+                    }
+                    float ha, hb, la, lb;
+                    acb::upk2(h2, ha, hb);
+                    acb::upk2(o2, la, lb);
+                    out[fa * L.fstride + id]    = ha;
+                    out[fb * L.fstride + id]    = hb;
+                    out_lo[fa * L.fstride + id] = la;
+                    out_lo[fb * L.fstride + id] = lb;
+                }
+            }
+#else
 #pragma unroll
             for (int f = 0; f < ACB_NF; ++f) {
-#if ACB_MIXED
-                float d = rkB * roc[f];
-                if (STEP > 0)
-                    d += rkA * ((cur[f] - cv.prev[f]) + (cv.cur_lo[f] - cv.prev_lo[f]));
-                float hi, lo;
-                acb::pair_add(cur[f], cv.cur_lo[f], d, hi, lo);
-                if (STEP == 3 && f >= 1 && f <= 3)
-                    acb::pair_add(hi, lo, fo[f - 1], hi, lo);
-                out[f * L.fstride + id]    = hi;
-                out_lo[f * L.fstride + id] = lo;
-#else
                 T r;
                 if (STEP == 0)
                     r = cur[f] + rkB * roc[f];
@@ -1007,8 +1064,8 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
                 if (STEP == 3 && f >= 1 && f <= 3)
                     r += fo[f - 1];
                 out[f * L.fstride + id] = r;
-#endif
             }
+#endif
         }
         __syncwarp();
         // with the queues the centre plane is done with; without them the

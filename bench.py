@@ -648,6 +648,7 @@ def run_ours(args) -> None:
     n = args.n
     host = host_mesh("mixed", n)
     dev = Device("mixed", host.info, gpu)
+    tile_config = dev.solve_config()[2]  # chosen by the autotuner at creation
     dev.load_mesh(host)
     res = timed_steps(dev, args.steps, args.warmup, ranks, sample_clocks=True, gpu_index=gpu)
     value = ranks.throughput(n ** 3, args.steps, res["total_ms"])  # total_ms: max over ranks
@@ -729,7 +730,7 @@ def run_ours(args) -> None:
                 "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak,
                              "unit": "GB/s", "frac": achieved_gbs / peak,
                              "traffic": traffic, "peak_source": peak_kind,
-                             "kernel": "solve_kernel (mixed)",
+                             "kernel": f"solve_kernel (mixed, {tile_config})",
                              "alg_bytes_per_cell_step": alg // n ** 3,
                              "solve_ms_per_substep": res["solve_ms_per_substep"]},
                 "clocks": res["clocks"], "gpu_launches": res["launches"],
