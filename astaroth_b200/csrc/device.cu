@@ -83,6 +83,7 @@ struct device_s {
 
     double* xfer; // device staging buffer for the double-precision views
     size_t xfer_elems;
+    StageBuf stage; // staging buffer of mesh loads
 
     unsigned* status;
     int solve_cfg;
@@ -546,11 +547,81 @@ for_each_row_run(const Layout& L, size_t s, size_t count, F fn)
     return AC_SUCCESS;
 }
 
+// Scatters n consecutive values of a field in reference order, starting at
+// flat index s, from a staging buffer into the padded layout (and zeroes
+// their lo parts when given: fresh values carry none).
+__global__ void
+scatter_rows_kernel(const Layout L, state_t* __restrict__ field, float* __restrict__ lo,
+                    const state_t* __restrict__ flat, unsigned long long s, unsigned long long n)
+{
+    const unsigned long long mx = (unsigned long long)L.mx;
+    for (unsigned long long u = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+         u += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long idx = s + u, row = idx / mx;
+        const long long dev = (long long)L.offx + (long long)row * L.mxp + (long long)(idx - row * mx);
+        field[dev] = flat[u];
+        if (lo)
+            lo[dev] = 0.f;
+    }
+}
+
+AcResult
+acb_host::stage_create(StageBuf* stage, size_t max_elems)
+{
+    const size_t cap = ((size_t)64 << 20) / sizeof(state_t);
+    stage->elems     = std::max<size_t>(1, std::min(max_elems, cap));
+    stage->buf       = nullptr;
+    stage->done      = nullptr;
+    ACB_CUDA_CHECK(cudaMalloc((void**)&stage->buf, stage->elems * sizeof(state_t)));
+    ACB_CUDA_CHECK(cudaEventCreateWithFlags(&stage->done, cudaEventDisableTiming));
+    return AC_SUCCESS;
+}
+
+void
+acb_host::stage_destroy(StageBuf* stage)
+{
+    if (stage->buf)
+        cudaFree(stage->buf);
+    if (stage->done)
+        cudaEventDestroy(stage->done);
+    stage->buf  = nullptr;
+    stage->done = nullptr;
+}
+
 AcResult
 acb_host::copy_field_range(cudaStream_t st, const Layout& L, state_t* field, size_t s,
-                           AcReal* host, size_t count, bool h2d, float* lo_field)
+                           AcReal* host, size_t count, bool h2d, float* lo_field,
+                           StageBuf* stage)
 {
     const size_t w   = sizeof(state_t);
+    if (h2d && stage && stage->buf) {
+        const size_t total = (size_t)L.mx * L.my * L.mz;
+        if (s > total || count > total - s) {
+            fprintf(stderr, "astaroth_b200: transfer range outside the mesh\n");
+            return AC_FAILURE;
+        }
+        if (count == 0)
+            return AC_SUCCESS;
+        ACB_CUDA_CHECK(cudaStreamWaitEvent(st, stage->done, 0));
+        for (size_t t = 0; t < count; t += stage->elems) {
+            const size_t n = std::min(stage->elems, count - t);
+            // cudaMemcpyDefault: the caller's mesh buffers are normally host
+            // memory, but a device-resident mesh is copied the same way
+            const cudaError_t err =
+                cudaMemcpyAsync(stage->buf, host + t, n * w, cudaMemcpyDefault, st);
+            if (err != cudaSuccess) {
+                fprintf(stderr, "astaroth_b200: transfer failed: %s\n", cudaGetErrorString(err));
+                return AC_FAILURE;
+            }
+            const int blocks = (int)std::min<size_t>((n + 255) / 256, 4096);
+            scatter_rows_kernel<<<blocks, 256, 0, st>>>(L, field, lo_field, stage->buf,
+                                                        (unsigned long long)(s + t),
+                                                        (unsigned long long)n);
+            ACB_CUDA_CHECK(cudaGetLastError());
+        }
+        ACB_CUDA_CHECK(cudaEventRecord(stage->done, st));
+        return AC_SUCCESS;
+    }
     const size_t dpw = (size_t)L.mxp * w, hpw = (size_t)L.mx * w;
     return for_each_row_run(L, s, count, [&](size_t dev, size_t t, size_t n, size_t rows) {
         // cudaMemcpyDefault: the caller's mesh buffers are normally host
@@ -866,6 +937,8 @@ acDeviceCreate(const int id, const AcMeshInfo config, Device* device_handle)
     ACB_CUDA_CHECK(cudaMallocHost((void**)&d->h_result, sizeof(double)));
     ACB_CUDA_CHECK(cudaMalloc((void**)&d->status, sizeof(unsigned)));
     ACB_CUDA_CHECK(cudaMemset(d->status, 0, sizeof(unsigned)));
+    if (stage_create(&d->stage, (size_t)d->L.mx * d->L.my * d->L.mz) != AC_SUCCESS)
+        return AC_FAILURE;
 
     acDeviceLoadDefaultUniforms(d);
     acDeviceLoadMeshInfo(d, config);
@@ -903,6 +976,7 @@ acDeviceDestroy(Device device)
     cudaFree(device->status);
     if (device->xfer)
         cudaFree(device->xfer);
+    stage_destroy(&device->stage);
     for (int i = 0; i < NUM_STREAMS; ++i)
         cudaStreamDestroy(device->streams[i]);
     free(device);
@@ -986,7 +1060,8 @@ acDeviceLoadVertexBufferWithOffset(const Device device, const Stream stream,
         return AC_FAILURE;
     return copy_field_range(stream_of(device, stream), L,
                             device->blk[device->cur] + h * L.fstride, didx,
-                            host_mesh.vertex_buffer[h] + sidx, (size_t)num_vertices, true, lo);
+                            host_mesh.vertex_buffer[h] + sidx, (size_t)num_vertices, true, lo,
+                            &device->stage);
 }
 
 AcResult
@@ -1050,7 +1125,7 @@ acDeviceStoreVertexBufferWithOffset(const Device device, const Stream stream,
     return copy_field_range(stream_of(device, stream), L,
                             device->blk[device->cur] + h * L.fstride, sidx,
                             host_mesh->vertex_buffer[h] + didx, (size_t)num_vertices, false,
-                            nullptr);
+                            nullptr, nullptr);
 }
 
 AcResult

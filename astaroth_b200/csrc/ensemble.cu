@@ -102,6 +102,7 @@ struct ensemble_s {
     int seg_planes; // target planes per z segment (0: whole columns)
     // ghost_ok[p]: the ghosts of every member's block p hold periodic images
     bool ghost_ok[2];
+    StageBuf stage; // staging buffer of member loads
 
     bool desc_valid;
     std::vector<MemberDesc<AcReal>> h_desc[2];
@@ -370,6 +371,13 @@ acEnsembleCreate(const int device_id, const int num_members, const AcMeshInfo* c
 #endif
         }
     }
+    size_t largest = 0;
+    for (const Member& mb : e->m)
+        largest = std::max(largest, (size_t)mb.L.mx * mb.L.my * mb.L.mz);
+    if (stage_create(&e->stage, largest) != AC_SUCCESS) {
+        acEnsembleDestroy(e);
+        return AC_FAILURE;
+    }
     for (int p = 0; p < 2; ++p) {
         ACB_CUDA_CHECK(cudaMalloc((void**)&e->d_desc[p], sizeof(MemberDesc<AcReal>) * num_members));
         ACB_CUDA_CHECK(cudaMalloc((void**)&e->d_halo[p], sizeof(HaloMember) * num_members));
@@ -405,6 +413,7 @@ acEnsembleDestroy(Ensemble e)
     }
     if (e->status)
         cudaFree(e->status);
+    stage_destroy(&e->stage);
     if (e->stream)
         cudaStreamDestroy(e->stream);
     delete e;
@@ -427,7 +436,7 @@ acEnsembleLoadMember(Ensemble e, const int member, const AcMesh host_mesh)
     for (int f = 0; f < NUM_VTXBUF_HANDLES; ++f) {
         float* lo = mb.lo[e->cur] ? mb.lo[e->cur] + f * mb.L.fstride : nullptr;
         if (copy_field_range(e->stream, mb.L, mb.blk[e->cur] + f * mb.L.fstride, 0,
-                             host_mesh.vertex_buffer[f], n, true, lo) != AC_SUCCESS)
+                             host_mesh.vertex_buffer[f], n, true, lo, &e->stage) != AC_SUCCESS)
             return AC_FAILURE;
     }
     ACB_CUDA_CHECK(cudaStreamSynchronize(e->stream));
@@ -448,7 +457,8 @@ acEnsembleStoreMember(Ensemble e, const int member, AcMesh* host_mesh)
     }
     for (int f = 0; f < NUM_VTXBUF_HANDLES; ++f)
         if (copy_field_range(e->stream, mb.L, mb.blk[e->cur] + f * mb.L.fstride, 0,
-                             host_mesh->vertex_buffer[f], n, false, nullptr) != AC_SUCCESS)
+                             host_mesh->vertex_buffer[f], n, false, nullptr, nullptr) !=
+            AC_SUCCESS)
             return AC_FAILURE;
     ACB_CUDA_CHECK(cudaStreamSynchronize(e->stream));
     return AC_SUCCESS;

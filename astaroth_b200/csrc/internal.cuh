@@ -96,9 +96,25 @@ SolveParams<AcReal> make_params(const AcMeshInfo& uniforms, const Layout& L, int
 // z segments per tile column so that tiles*segments fills the last wave best
 int choose_segments(long long ntiles, int nzr, long long slots, int min_planes);
 
+// Device staging buffer of loads: the caller's values are copied into it in
+// one contiguous transfer per chunk and a kernel scatters them into the padded
+// rows (a pitched host-to-device copy of rows a few KB long runs at about a
+// third of the contiguous rate). `done` is recorded after each use, and the
+// next use, on whatever stream, waits for it.
+struct StageBuf {
+    state_t* buf;
+    size_t elems;
+    cudaEvent_t done;
+};
+// a buffer of min(max_elems, 64 MB) values
+AcResult stage_create(StageBuf* stage, size_t max_elems);
+void stage_destroy(StageBuf* stage);
+
 // copies a flat range of a field between host memory (reference order) and
-// the padded device layout; zeroes the lo parts of loaded values when given
+// the padded device layout; zeroes the lo parts of loaded values when given.
+// Loads go through the staging buffer when one is given.
 AcResult copy_field_range(cudaStream_t st, const Layout& L, state_t* field, size_t s,
-                          AcReal* host, size_t count, bool h2d, float* lo_field);
+                          AcReal* host, size_t count, bool h2d, float* lo_field,
+                          StageBuf* stage);
 
 } // namespace acb_host

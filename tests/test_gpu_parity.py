@@ -586,3 +586,62 @@ def test_whole_box_fill_after_substep_is_exact(flavour, dims):
     for w in range(8):
         assert np.array_equal(first[w], init.wrap_ghosts(interior(first[w]))), w
         assert np.array_equal(first[w], second[w]), w
+
+
+@pytest.mark.parametrize("flavour", FLAVOURS)
+def test_staged_loads(flavour):
+    """Loads go through a device staging buffer (a contiguous copy per chunk,
+    then a scatter into the padded rows): a partial range loaded from one
+    offset of the host mesh to another of the device lands exactly there and
+    nowhere else; a field larger than one staging chunk (64 MB) loads whole;
+    and loaded values carry no lo part in the mixed build, even where the
+    block held a nonzero lo part before."""
+    prec = abi.PRECISIONS[flavour]
+    rng = np.random.default_rng(5)
+    nx, ny, nz = 37, 29, 23
+    info = abi.make_info(prec, nx, ny, nz)
+    shape = (nz + 6, ny + 6, nx + 6)
+    base = [rng.standard_normal(shape).astype(prec.np_dtype) for _ in range(8)]
+    new = [rng.standard_normal(shape).astype(prec.np_dtype) for _ in range(8)]
+    with new_device(flavour, info) as dev:
+        dev.load_mesh(abi.HostMesh(prec, info, base))
+        src_flat, dst_flat, count = 777, 2345, 4 * (nx + 6) + 29
+
+        def int3_of(flat):
+            k, rem = divmod(flat, (nx + 6) * (ny + 6))
+            j, i = divmod(rem, nx + 6)
+            return abi.int3(i, j, k)
+
+        src_mesh = abi.HostMesh(prec, info, new)
+        rc = dev.lib.acDeviceLoadVertexBufferWithOffset(dev.handle, 0, src_mesh.cmesh, 5,
+                                                        int3_of(src_flat), int3_of(dst_flat),
+                                                        count)
+        assert rc == 0
+        back = abi.HostMesh(prec, info)
+        dev.store_mesh(back)
+        want = base[5].reshape(-1).copy()
+        want[dst_flat:dst_flat + count] = new[5].reshape(-1)[src_flat:src_flat + count]
+        assert np.array_equal(back.fields[5].reshape(-1), want)
+        for w in (0, 1, 2, 3, 4, 6, 7):
+            assert np.array_equal(back.fields[w], base[w]), w
+
+        if flavour == "mixed":
+            # give both blocks nonzero lo parts, then load over them
+            for s in range(3):
+                dev.periodic_boundconds()
+                dev.integrate_substep(s, 1e-3)
+                dev.swap_buffers()
+            dev.load_mesh(abi.HostMesh(prec, info, new))
+            for w in range(8):
+                assert np.array_equal(dev.store_double(w), new[w].astype(np.float64)), w
+
+    n = 256  # 262^3 values per field: more than one staging chunk
+    info = abi.make_info(prec, n)
+    big = [rng.standard_normal((n + 6,) * 3).astype(prec.np_dtype) for _ in range(2)]
+    fields = [big[w % 2] for w in range(8)]
+    with new_device(flavour, info) as dev:
+        dev.load_mesh(abi.HostMesh(prec, info, fields))
+        back = abi.HostMesh(prec, info)
+        dev.store_mesh(back)
+        for w in range(8):
+            assert np.array_equal(back.fields[w], fields[w]), w
