@@ -275,6 +275,22 @@ acb_host::make_params(const AcMeshInfo& uniforms, const Layout& L, int step, int
     for (int p = 0; p < 3; ++p)
         for (int k = 0; k < 3; ++k)
             P.cx[p][k] = (AcReal)(cx[k] * inv[pa[p]] * inv[pb[p]]);
+    if (sizeof(AcReal) == 4) {
+        // the same coefficients as (c, c) lane pairs for the packed stencil sums
+        auto dup = [](AcReal c) {
+            uint32_t b;
+            memcpy(&b, &c, 4);
+            return ((unsigned long long)b << 32) | b;
+        };
+        for (int a = 0; a < 3; ++a) {
+            for (int k = 0; k < 3; ++k)
+                P.c1p[a][k] = dup(P.c1[a][k]);
+            for (int k = 0; k < 4; ++k)
+                P.c2p[a][k] = dup(P.c2[a][k]);
+        }
+        for (int k = 0; k < 3; ++k)
+            P.cxp[k] = dup(P.cx[0][k]);
+    }
 
     const double gamma = rp[AC_gamma], cp = rp[AC_cp_sound], mu0 = rp[AC_mu0];
     P.nu           = rp[AC_nu_visc];

@@ -45,6 +45,9 @@ struct SolveParams {
     T c1[3][3];   // first derivative: axis, k-1; pre-scaled by 1/ds
     T c2[3][4];   // second derivative: axis, {centre, k=1..3}; pre-scaled by 1/ds^2
     T cx[3][3];   // diagonal cross derivative: pair {xy, xz, yz}, k-1; pre-scaled
+    // single precision: c1, c2 and the xy row of cx as (c, c) pairs of FP32
+    // lanes, the coefficient operands of packed sums over two fields
+    unsigned long long c1p[3][3], c2p[3][4], cxp[3];
     T nu, eta, inv_mu0, eta_mu0, zeta;
     T cs2_sound, inv_cp, gamma, gm1, gamma_inv_cp, lnrho0, lnT0, k_heat;
     T rkA, rkB; // out = cur + rkA * (cur - prev) + rkB * rate; rkA unused at s = 0
@@ -384,6 +387,22 @@ sub2(F2 a, F2 b)
     return r;
 }
 
+__device__ __forceinline__ F2
+mul2(F2 a, F2 b)
+{
+    F2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+
+__device__ __forceinline__ F2
+fma2(F2 a, F2 b, F2 c)
+{
+    F2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return r;
+}
+
 template <bool GX_, bool GY_, bool GZ_, bool XY_, bool XZ_, bool YZ_>
 struct DFlags {
     static constexpr bool GX = GX_, GY = GY_, GZ = GZ_, XY = XY_, XZ = XZ_, YZ = YZ_;
@@ -469,77 +488,85 @@ pair_derivs_q(const float* __restrict__ cA, const float* __restrict__ cB, const 
     rA.v        = a0;
     rB.v        = b0;
     const F2 F0 = pk2(a0, b0);
-    float dxA[3], dxB[3], sxA[3], sxB[3], dyA[3], dyB[3], syA[3], syB[3], dzA[3], dzB[3],
-        szA[3], szB[3];
+    F2 DX[3], SX[3], DY[3], SY[3], DZ[3], SZ[3];
     // Second differences as u + v with u = f(+k) - f0, v = f(-k) - f0: for a
     // smooth field u and v are exact in FP32 (Sterbenz), so f(+k) + f(-k) - 2 f0
     // keeps its digits instead of cancelling terms of size |c0 f0| (about
     // 2.7 f / ds^2); mathematically the same stencil (c0 = -2 (c1 + c2 + c3)).
     // First differences f(+k) - f(-k) directly, as prime_queue forms the queued
     // ones, so results do not depend on where a task's z segment starts.
-    auto dsum = [&](F2 p, F2 m, float& dA, float& dB, float& sA, float& sB) {
-        upk2(sub2(p, m), dA, dB);
-        upk2(add2(sub2(p, F0), sub2(m, F0)), sA, sB);
+    auto dsum = [&](F2 p, F2 m, F2& D, F2& S) {
+        D = sub2(p, m);
+        S = add2(sub2(p, F0), sub2(m, F0));
     };
 #pragma unroll
     for (int k = 1; k <= 3; ++k) {
-        dsum(pk2(cA[k], cB[k]), pk2(cA[-k], cB[-k]), dxA[k - 1], dxB[k - 1], sxA[k - 1],
-             sxB[k - 1]);
-        dsum(pk2(cA[k * BX], cB[k * BX]), pk2(cA[-k * BX], cB[-k * BX]), dyA[k - 1], dyB[k - 1],
-             syA[k - 1], syB[k - 1]);
+        dsum(pk2(cA[k], cB[k]), pk2(cA[-k], cB[-k]), DX[k - 1], SX[k - 1]);
+        dsum(pk2(cA[k * BX], cB[k * BX]), pk2(cA[-k * BX], cB[-k * BX]), DY[k - 1], SY[k - 1]);
     }
-    dsum(pk2(cA[zo[4]], cB[zo[4]]), pk2(QA.v1, QB.v1), dzA[0], dzB[0], szA[0], szB[0]);
-    dsum(pk2(cA[zo[5]], cB[zo[5]]), pk2(QA.v2, QB.v2), dzA[1], dzB[1], szA[1], szB[1]);
-    dsum(pk2(cA[zo[6]], cB[zo[6]]), pk2(QA.v3, QB.v3), dzA[2], dzB[2], szA[2], szB[2]);
-    auto first = [&](const float* c1, const float* d) { return c1[0] * d[0] + c1[1] * d[1] + c1[2] * d[2]; };
-    auto second = [&](const float* c2, float, const float* s) {
-        return c2[1] * s[0] + c2[2] * s[1] + c2[3] * s[2];
+    dsum(pk2(cA[zo[4]], cB[zo[4]]), pk2(QA.v1, QB.v1), DZ[0], SZ[0]);
+    dsum(pk2(cA[zo[5]], cB[zo[5]]), pk2(QA.v2, QB.v2), DZ[1], SZ[1]);
+    dsum(pk2(cA[zo[6]], cB[zo[6]]), pk2(QA.v3, QB.v3), DZ[2], SZ[2]);
+    // Coefficient sums sum_k c_k d_k of both fields. The FP32 build forms them
+    // in packed lanes ((c, c) coefficient pairs; 2-3 % faster per step at
+    // 512^3); the mixed build, whose update holds more registers, runs 2 %
+    // faster with them in scalar form (the same operations per lane).
+    constexpr bool PACKED_SUMS = !ACB_MIXED;
+    auto sum3 = [&](const unsigned long long* cp, const float* c, const F2* d, float& oa,
+                    float& ob) {
+        if constexpr (PACKED_SUMS) {
+            F2 r = mul2(F2{cp[0]}, d[0]);
+            r    = fma2(F2{cp[1]}, d[1], r);
+            upk2(fma2(F2{cp[2]}, d[2], r), oa, ob);
+        }
+        else {
+            float a[3], b[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                upk2(d[k], a[k], b[k]);
+            oa = c[0] * a[0] + c[1] * a[1] + c[2] * a[2];
+            ob = c[0] * b[0] + c[1] * b[1] + c[2] * b[2];
+        }
     };
-    if (FA::GX) rA.gx = first(P.c1[0], dxA);
-    if (FB::GX) rB.gx = first(P.c1[0], dxB);
-    if (FA::GY) rA.gy = first(P.c1[1], dyA);
-    if (FB::GY) rB.gy = first(P.c1[1], dyB);
-    if (FA::GZ) rA.gz = first(P.c1[2], dzA);
-    if (FB::GZ) rB.gz = first(P.c1[2], dzB);
-    rA.xx = second(P.c2[0], a0, sxA);
-    rB.xx = second(P.c2[0], b0, sxB);
-    rA.yy = second(P.c2[1], a0, syA);
-    rB.yy = second(P.c2[1], b0, syB);
-    rA.zz = second(P.c2[2], a0, szA);
-    rB.zz = second(P.c2[2], b0, szB);
+    float gA, gB;
+    if (FA::GX || FB::GX) {
+        sum3(P.c1p[0], P.c1[0], DX, gA, gB);
+        if (FA::GX) rA.gx = gA;
+        if (FB::GX) rB.gx = gB;
+    }
+    if (FA::GY || FB::GY) {
+        sum3(P.c1p[1], P.c1[1], DY, gA, gB);
+        if (FA::GY) rA.gy = gA;
+        if (FB::GY) rB.gy = gB;
+    }
+    if (FA::GZ || FB::GZ) {
+        sum3(P.c1p[2], P.c1[2], DZ, gA, gB);
+        if (FA::GZ) rA.gz = gA;
+        if (FB::GZ) rB.gz = gB;
+    }
+    sum3(P.c2p[0] + 1, P.c2[0] + 1, SX, rA.xx, rB.xx);
+    sum3(P.c2p[1] + 1, P.c2[1] + 1, SY, rA.yy, rB.yy);
+    sum3(P.c2p[2] + 1, P.c2[2] + 1, SZ, rA.zz, rB.zz);
+    // the x and y differences of this plane, for the z-diagonal queues
+    float dxA[3], dxB[3], dyA[3], dyB[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        upk2(DX[k], dxA[k], dxB[k]);
+        upk2(DY[k], dyA[k], dyB[k]);
+    }
 
     // xy diagonals (the whole stencil from the centre plane)
     if (FA::XY || FB::XY) {
-        float eA[3], eB[3];
+        static_assert(FA::XY == FB::XY, "xy diagonals are formed for both fields of a pair");
+        F2 E[3];
 #pragma unroll
         for (int k = 1; k <= 3; ++k) {
             const int pp = k + k * BX, mm = -k - k * BX, pm = k - k * BX, mp = -k + k * BX;
-            if (FA::XY && FB::XY) {
-                const F2 a = add2(pk2(cA[pp], cB[pp]), pk2(cA[mm], cB[mm]));
-                const F2 b = add2(pk2(cA[pm], cB[pm]), pk2(cA[mp], cB[mp]));
-                upk2(sub2(a, b), eA[k - 1], eB[k - 1]);
-            }
-            else if (FA::XY) {
-                eA[k - 1] = (cA[pp] + cA[mm]) - (cA[pm] + cA[mp]);
-            }
-            else {
-                eB[k - 1] = (cB[pp] + cB[mm]) - (cB[pm] + cB[mp]);
-            }
+            const F2 a = add2(pk2(cA[pp], cB[pp]), pk2(cA[mm], cB[mm]));
+            const F2 b = add2(pk2(cA[pm], cB[pm]), pk2(cA[mp], cB[mp]));
+            E[k - 1]   = sub2(a, b);
         }
-        if (FA::XY) {
-            float s = 0;
-            s += P.cx[0][0] * eA[0];
-            s += P.cx[0][1] * eA[1];
-            s += P.cx[0][2] * eA[2];
-            rA.xy = s;
-        }
-        if (FB::XY) {
-            float s = 0;
-            s += P.cx[0][0] * eB[0];
-            s += P.cx[0][1] * eB[1];
-            s += P.cx[0][2] * eB[2];
-            rB.xy = s;
-        }
+        sum3(P.cxp, P.cx[0], E, rA.xy, rB.xy);
     }
 
     // z diagonals: the first of A's with the first of B's, the second with the second
@@ -777,22 +804,6 @@ pair_add(float hi, float lo, float d, float& ohi, float& olo)
     const float l  = lo + e;
     ohi            = s + l; // renormalise
     olo            = l - (ohi - s);
-}
-
-__device__ __forceinline__ F2
-mul2(F2 a, F2 b)
-{
-    F2 r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-    return r;
-}
-
-__device__ __forceinline__ F2
-fma2(F2 a, F2 b, F2 c)
-{
-    F2 r;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
-    return r;
 }
 
 // pair_add of two fields in packed lanes (the same operations lane by lane).
