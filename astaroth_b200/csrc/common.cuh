@@ -24,10 +24,17 @@
 typedef AcReal state_t;
 
 // ---------------------------------------------------------------------------
-// Device memory layout of one field block (8 fields contiguous).
+// Device memory layout of one field block: ACB_NARR arrays of 8-byte elements,
+// one element per vertex.
+//   FP64 build: eight arrays, array f = field f (a double per vertex).
+//   FP32 and mixed builds: four arrays of interleaved field pairs, (lnrho, ss),
+//     (ux, ax), (uy, ay), (uz, az): element = (field A, field B) as two floats,
+//     so one 8-byte load brings a stencil point of both fields of a pair (the
+//     pairs are the fields whose stencils have the same shape). The mixed
+//     build's lo parts use the same layout.
 //
-// Field f, vertex (i, j, k) with i in [0, mx), j in [0, my), k in [0, mz):
-//     block + f * fstride + offx + i + j * mxp + k * mxp * my
+// Element of vertex (i, j, k), i in [0, mx), j in [0, my), k in [0, mz), of
+// array a:  block + a * fstride + offx + i + j * mxp + k * mxp * my  (elements)
 // - mxp (row pitch) is a multiple of 32 bytes and >= offx + mx;
 // - offx puts the first interior vertex (i = 3) of every row on a 32-byte
 //   (one DRAM sector) boundary, so rows of interior stores are whole sectors;
@@ -35,17 +42,40 @@ typedef AcReal state_t;
 // The row pitch is the reason for the padding: TMA needs every global stride to
 // be a multiple of 16 bytes, and mx = n + 6 is not in general.
 // ---------------------------------------------------------------------------
+#define ACB_PAIRED (sizeof(state_t) == 4)
+static constexpr int ACB_NARR  = ACB_PAIRED ? 4 : ACB_NF; // arrays of a block
+static constexpr int ACB_LANES = ACB_PAIRED ? 2 : 1;      // state values per element
+static constexpr int ACB_ELEM  = 8;                       // bytes per element
+
+// array and lane of field f (lnrho 0, ux 1, uy 2, uz 3, ax 4, ay 5, az 6, ss 7)
+__host__ __device__ constexpr int
+acb_array(int f)
+{
+    return ACB_PAIRED ? (f < 4 ? f : (f == 7 ? 0 : f - 3)) : f;
+}
+__host__ __device__ constexpr int
+acb_lane(int f)
+{
+    return ACB_PAIRED ? (f < 4 ? 0 : 1) : 0;
+}
+// the field held in lane l of array a
+__host__ __device__ constexpr int
+acb_field(int a, int l)
+{
+    return ACB_PAIRED ? (l == 0 ? a : (a == 0 ? 7 : a + 3)) : a;
+}
+
 struct Layout {
     int mx, my, mz;    // logical extents (n + 6)
     int nx, ny, nz;    // interior extents
     int mxp;           // row pitch, elements
     int offx;          // leading offset, elements
     long long plane;   // mxp * my
-    long long fstride; // elements between fields
+    long long fstride; // elements between arrays
 };
 
 static inline Layout
-make_layout(int nx, int ny, int nz, int elem_bytes)
+make_layout(int nx, int ny, int nz)
 {
     Layout L;
     L.nx = nx;
@@ -54,19 +84,36 @@ make_layout(int nx, int ny, int nz, int elem_bytes)
     L.mx = nx + 2 * NGHOST;
     L.my = ny + 2 * NGHOST;
     L.mz = nz + 2 * NGHOST;
-    const int sector = 32 / elem_bytes; // elements per 32-byte sector
+    const int sector = 32 / ACB_ELEM; // elements per 32-byte sector
     L.offx           = sector - NGHOST;
     L.mxp            = ((L.offx + L.mx + sector - 1) / sector) * sector;
     L.plane          = (long long)L.mxp * L.my;
-    const long long q = 256 / elem_bytes;
+    const long long q = 256 / ACB_ELEM;
     L.fstride         = ((L.offx + L.plane * L.mz + q - 1) / q) * q;
     return L;
+}
+
+// bytes of one block (hi, or the lo parts in the mixed build)
+static inline size_t
+block_bytes(const Layout& L)
+{
+    return (size_t)L.fstride * ACB_NARR * ACB_ELEM;
 }
 
 __host__ __device__ __forceinline__ long long
 lidx(const Layout& L, int i, int j, int k)
 {
     return (long long)L.offx + i + (long long)j * L.mxp + (long long)k * L.plane;
+}
+
+// Offset, in state values (floats or doubles), of field f at the element
+// index id of a vertex (lidx): the field's value there is block[fidx(L, f, id)].
+// A field's values are ACB_LANES apart: block + fidx(L, f, 0) is the field's
+// base and its vertex id sits at base[id * ACB_LANES].
+__host__ __device__ __forceinline__ long long
+fidx(const Layout& L, int f, long long id)
+{
+    return ((long long)acb_array(f) * L.fstride + id) * ACB_LANES + acb_lane(f);
 }
 
 // Status bits a kernel may raise in the per-device status word.

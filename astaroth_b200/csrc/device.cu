@@ -145,15 +145,16 @@ acb_host::encode_block_map(const Layout& L, const state_t* block, const SolveCon
         fprintf(stderr, "astaroth_b200: cuTensorMapEncodeTiled unavailable\n");
         return AC_FAILURE;
     }
-    const cuuint64_t esz     = sizeof(state_t);
-    const cuuint64_t dim[4]  = {(cuuint64_t)L.mxp, (cuuint64_t)L.my, (cuuint64_t)L.mz, ACB_NF};
+    // the block's arrays of 8-byte elements (a field pair or a double); the
+    // copy moves bits, so FLOAT64 serves both layouts
+    const cuuint64_t esz     = ACB_ELEM;
+    const cuuint64_t dim[4]  = {(cuuint64_t)L.mxp, (cuuint64_t)L.my, (cuuint64_t)L.mz, ACB_NARR};
     const cuuint64_t str[3]  = {(cuuint64_t)L.mxp * esz, (cuuint64_t)L.plane * esz,
                                (cuuint64_t)L.fstride * esz};
     const cuuint32_t box[4]  = {(cuuint32_t)(cfg.TX + 8), (cuuint32_t)(cfg.TY + 2 * NGHOST), 1,
-                               ACB_NF};
+                               ACB_NARR};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
-    const CUtensorMapDataType dt = sizeof(state_t) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
-                                                        : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
     CUresult r = enc(map, dt, 4, (void*)block, dim, str, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -173,13 +174,13 @@ acb_host::encode_centre_map(const Layout& L, const void* block, const SolveConfi
         fprintf(stderr, "astaroth_b200: cuTensorMapEncodeTiled unavailable\n");
         return AC_FAILURE;
     }
-    const cuuint64_t esz     = 4;
-    const cuuint64_t dim[4]  = {(cuuint64_t)L.mxp, (cuuint64_t)L.my, (cuuint64_t)L.mz, ACB_NF};
+    const cuuint64_t esz     = ACB_ELEM;
+    const cuuint64_t dim[4]  = {(cuuint64_t)L.mxp, (cuuint64_t)L.my, (cuuint64_t)L.mz, ACB_NARR};
     const cuuint64_t str[3]  = {(cuuint64_t)L.mxp * esz, (cuuint64_t)L.plane * esz,
                                (cuuint64_t)L.fstride * esz};
-    const cuuint32_t box[4]  = {(cuuint32_t)cfg.TX, (cuuint32_t)cfg.TY, 1, ACB_NF};
+    const cuuint32_t box[4]  = {(cuuint32_t)cfg.TX, (cuuint32_t)cfg.TY, 1, ACB_NARR};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(block), dim, str,
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(block), dim, str,
                      box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
@@ -507,8 +508,8 @@ run_reduce(const Device d, cudaStream_t st, int rtype, int nin, const int* handl
     for (int w = 0; w < nin; ++w) {
         if (handles[w] < 0 || handles[w] >= NUM_VTXBUF_HANDLES)
             return AC_FAILURE;
-        a.f[w]  = d->blk[d->cur] + handles[w] * L.fstride;
-        a.lo[w] = d->lo[d->cur] ? d->lo[d->cur] + handles[w] * L.fstride : nullptr;
+        a.f[w]  = d->blk[d->cur] + fidx(L, handles[w], 0);
+        a.lo[w] = d->lo[d->cur] ? d->lo[d->cur] + fidx(L, handles[w], 0) : nullptr;
     }
     a.nin      = nin;
     a.rtype    = rtype;
@@ -530,55 +531,39 @@ run_reduce(const Device d, cudaStream_t st, int rtype, int nin, const int* handl
     return AC_SUCCESS;
 }
 
-// Visits the rows of a flat range [s, s + count) of logical indices of a field
-// (reference order, rows of mx): fn(dev_offset_elems, flat_offset, n_elems, n_rows)
-// with n_rows > 1 only for runs of whole rows.
-template <class F>
-static AcResult
-for_each_row_run(const Layout& L, size_t s, size_t count, F fn)
+// Element index (lidx) of the vertex at flat reference-order index idx.
+__device__ __forceinline__ long long
+flat_to_elem(const Layout& L, unsigned long long idx)
 {
-    const size_t mx = (size_t)L.mx;
-    const size_t total = (size_t)L.mx * L.my * L.mz;
-    if (s > total || count > total - s) {
-        fprintf(stderr, "astaroth_b200: transfer range outside the mesh\n");
-        return AC_FAILURE;
-    }
-    size_t t = 0;
-    while (t < count) {
-        const size_t idx = s + t, row = idx / mx, i = idx % mx;
-        const size_t dev = (size_t)L.offx + row * (size_t)L.mxp + i;
-        if (i != 0 || count - t < mx) {
-            const size_t n = std::min(mx - i, count - t);
-            if (fn(dev, t, n, (size_t)1) != AC_SUCCESS)
-                return AC_FAILURE;
-            t += n;
-        }
-        else {
-            const size_t rows = (count - t) / mx;
-            if (fn(dev, t, mx, rows) != AC_SUCCESS)
-                return AC_FAILURE;
-            t += rows * mx;
-        }
-    }
-    return AC_SUCCESS;
+    const unsigned long long mx = (unsigned long long)L.mx, row = idx / mx;
+    return (long long)L.offx + (long long)row * L.mxp + (long long)(idx - row * mx);
 }
 
-// Scatters n consecutive values of a field in reference order, starting at
-// flat index s, from a staging buffer into the padded layout (and zeroes
-// their lo parts when given: fresh values carry none).
+// Scatters n consecutive values of a field (field: its base, fidx(L, f, 0)) in
+// reference order, starting at flat index s, from a staging buffer into the
+// padded layout (and zeroes their lo parts when given: fresh values carry none).
 __global__ void
 scatter_rows_kernel(const Layout L, state_t* __restrict__ field, float* __restrict__ lo,
                     const state_t* __restrict__ flat, unsigned long long s, unsigned long long n)
 {
-    const unsigned long long mx = (unsigned long long)L.mx;
     for (unsigned long long u = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; u < n;
          u += (unsigned long long)gridDim.x * blockDim.x) {
-        const unsigned long long idx = s + u, row = idx / mx;
-        const long long dev = (long long)L.offx + (long long)row * L.mxp + (long long)(idx - row * mx);
-        field[dev] = flat[u];
+        const long long dev = flat_to_elem(L, s + u) * ACB_LANES;
+        field[dev]          = flat[u];
         if (lo)
             lo[dev] = 0.f;
     }
+}
+
+// The reverse: n values of a field from the padded layout into a staging
+// buffer in reference order.
+__global__ void
+gather_rows_kernel(const Layout L, const state_t* __restrict__ field, state_t* __restrict__ flat,
+                   unsigned long long s, unsigned long long n)
+{
+    for (unsigned long long u = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+         u += (unsigned long long)gridDim.x * blockDim.x)
+        flat[u] = field[flat_to_elem(L, s + u) * ACB_LANES];
 }
 
 AcResult
@@ -609,58 +594,49 @@ acb_host::copy_field_range(cudaStream_t st, const Layout& L, state_t* field, siz
                            AcReal* host, size_t count, bool h2d, float* lo_field,
                            StageBuf* stage)
 {
-    const size_t w   = sizeof(state_t);
-    if (h2d && stage && stage->buf) {
-        const size_t total = (size_t)L.mx * L.my * L.mz;
-        if (s > total || count > total - s) {
-            fprintf(stderr, "astaroth_b200: transfer range outside the mesh\n");
-            return AC_FAILURE;
-        }
-        if (count == 0)
-            return AC_SUCCESS;
-        ACB_CUDA_CHECK(cudaStreamWaitEvent(st, stage->done, 0));
-        for (size_t t = 0; t < count; t += stage->elems) {
-            const size_t n = std::min(stage->elems, count - t);
-            // cudaMemcpyDefault: the caller's mesh buffers are normally host
-            // memory, but a device-resident mesh is copied the same way
-            const cudaError_t err =
-                cudaMemcpyAsync(stage->buf, host + t, n * w, cudaMemcpyDefault, st);
-            if (err != cudaSuccess) {
-                fprintf(stderr, "astaroth_b200: transfer failed: %s\n", cudaGetErrorString(err));
-                return AC_FAILURE;
-            }
-            const int blocks = (int)std::min<size_t>((n + 255) / 256, 4096);
-            scatter_rows_kernel<<<blocks, 256, 0, st>>>(L, field, lo_field, stage->buf,
-                                                        (unsigned long long)(s + t),
-                                                        (unsigned long long)n);
-            ACB_CUDA_CHECK(cudaGetLastError());
-        }
-        ACB_CUDA_CHECK(cudaEventRecord(stage->done, st));
-        return AC_SUCCESS;
+    const size_t w     = sizeof(state_t);
+    const size_t total = (size_t)L.mx * L.my * L.mz;
+    if (s > total || count > total - s) {
+        fprintf(stderr, "astaroth_b200: transfer range outside the mesh\n");
+        return AC_FAILURE;
     }
-    const size_t dpw = (size_t)L.mxp * w, hpw = (size_t)L.mx * w;
-    return for_each_row_run(L, s, count, [&](size_t dev, size_t t, size_t n, size_t rows) {
+    if (count == 0)
+        return AC_SUCCESS;
+    if (!stage || !stage->buf) {
+        fprintf(stderr, "astaroth_b200: transfer without a staging buffer\n");
+        return AC_FAILURE;
+    }
+    ACB_CUDA_CHECK(cudaStreamWaitEvent(st, stage->done, 0));
+    for (size_t t = 0; t < count; t += stage->elems) {
+        const size_t n   = std::min(stage->elems, count - t);
+        const int blocks = (int)std::min<size_t>((n + 255) / 256, 4096);
         // cudaMemcpyDefault: the caller's mesh buffers are normally host
-        // memory, but a device-resident mesh (unified addressing) is copied
-        // device to device the same way
+        // memory, but a device-resident mesh is copied the same way
         cudaError_t err;
-        if (rows == 1)
-            err = h2d ? cudaMemcpyAsync(field + dev, host + t, n * w, cudaMemcpyDefault, st)
-                      : cudaMemcpyAsync(host + t, field + dev, n * w, cudaMemcpyDefault, st);
-        else
-            err = h2d ? cudaMemcpy2DAsync(field + dev, dpw, host + t, hpw, n * w, rows,
-                                          cudaMemcpyDefault, st)
-                      : cudaMemcpy2DAsync(host + t, hpw, field + dev, dpw, n * w, rows,
-                                          cudaMemcpyDefault, st);
-        if (err == cudaSuccess && h2d && lo_field) // fresh values carry no lo part
-            err = cudaMemset2DAsync(lo_field + dev, (size_t)L.mxp * sizeof(float), 0,
-                                    n * sizeof(float), rows, st);
+        if (h2d) {
+            err = cudaMemcpyAsync(stage->buf, host + t, n * w, cudaMemcpyDefault, st);
+            if (err == cudaSuccess) {
+                scatter_rows_kernel<<<blocks, 256, 0, st>>>(L, field, lo_field, stage->buf,
+                                                            (unsigned long long)(s + t),
+                                                            (unsigned long long)n);
+                err = cudaGetLastError();
+            }
+        }
+        else {
+            gather_rows_kernel<<<blocks, 256, 0, st>>>(L, field, stage->buf,
+                                                       (unsigned long long)(s + t),
+                                                       (unsigned long long)n);
+            err = cudaGetLastError();
+            if (err == cudaSuccess)
+                err = cudaMemcpyAsync(host + t, stage->buf, n * w, cudaMemcpyDefault, st);
+        }
         if (err != cudaSuccess) {
             fprintf(stderr, "astaroth_b200: transfer failed: %s\n", cudaGetErrorString(err));
             return AC_FAILURE;
         }
-        return AC_SUCCESS;
-    });
+    }
+    ACB_CUDA_CHECK(cudaEventRecord(stage->done, st));
+    return AC_SUCCESS;
 }
 
 // flat (reference-order) double <-> padded field, for the double views and fills
@@ -673,7 +649,7 @@ pack_kernel(const Layout L, state_t* __restrict__ field, float* __restrict__ lo,
          t += (long long)gridDim.x * blockDim.x) {
         const long long row = t / L.mx;
         const int i         = (int)(t - row * L.mx);
-        const long long id  = L.offx + row * L.mxp + i;
+        const long long id  = (L.offx + row * L.mxp + i) * ACB_LANES;
         if (to_flat) {
             double v = (double)field[id];
             if (ACB_MIXED && lo)
@@ -697,8 +673,8 @@ launch_pack(const Device d, cudaStream_t st, int blk, int handle, double* flat, 
     const Layout& L = d->L;
     if (ensure_lo_ghosts(d, st, blk) != AC_SUCCESS)
         return AC_FAILURE;
-    state_t* f      = d->blk[blk] + handle * L.fstride;
-    float* lo       = d->lo[blk] ? d->lo[blk] + handle * L.fstride : nullptr;
+    state_t* f      = d->blk[blk] + fidx(L, handle, 0);
+    float* lo       = d->lo[blk] ? d->lo[blk] + fidx(L, handle, 0) : nullptr;
     pack_kernel<<<d->num_sms * 8, 256, 0, st>>>(L, f, lo, flat, to_flat, fill, value);
     ACB_CUDA_CHECK(cudaGetLastError());
     d->launches++;
@@ -935,14 +911,14 @@ acDeviceCreate(const int id, const AcMeshInfo config, Device* device_handle)
         ACB_CUDA_CHECK(cudaStreamCreateWithPriority(&d->streams[i], cudaStreamNonBlocking, prio));
     }
 
-    d->L               = make_layout(nx, ny, nz, (int)sizeof(state_t));
-    const size_t bytes = (size_t)d->L.fstride * ACB_NF * sizeof(state_t);
+    d->L               = make_layout(nx, ny, nz);
+    const size_t bytes = block_bytes(d->L);
     for (int b = 0; b < 2; ++b) {
         ACB_CUDA_CHECK(cudaMalloc((void**)&d->blk[b], bytes));
         ACB_CUDA_CHECK(cudaMemset(d->blk[b], 0, bytes));
 #if ACB_MIXED
-        ACB_CUDA_CHECK(cudaMalloc((void**)&d->lo[b], (size_t)d->L.fstride * ACB_NF * sizeof(float)));
-        ACB_CUDA_CHECK(cudaMemset(d->lo[b], 0, (size_t)d->L.fstride * ACB_NF * sizeof(float)));
+        ACB_CUDA_CHECK(cudaMalloc((void**)&d->lo[b], block_bytes(d->L)));
+        ACB_CUDA_CHECK(cudaMemset(d->lo[b], 0, block_bytes(d->L)));
 #endif
     }
     d->red_max_blocks = d->num_sms * 8;
@@ -1011,7 +987,7 @@ acDeviceAutoOptimize(const Device device)
     const int3 s          = make_int3(NGHOST, NGHOST, NGHOST);
     const int3 e = make_int3(NGHOST + device->L.nx, NGHOST + device->L.ny, NGHOST + device->L.nz);
     // keep the out block (the substep overwrites it)
-    const size_t bytes = (size_t)device->L.fstride * ACB_NF * sizeof(state_t);
+    const size_t bytes = block_bytes(device->L);
     state_t* save      = nullptr;
     ACB_CUDA_CHECK(cudaMalloc((void**)&save, bytes));
     ACB_CUDA_CHECK(cudaMemcpyAsync(save, device->blk[device->cur ^ 1], bytes,
@@ -1070,12 +1046,12 @@ acDeviceLoadVertexBufferWithOffset(const Device device, const Stream stream,
     const size_t sidx = acVertexBufferIdx(src.x, src.y, src.z, host_mesh.info);
     const size_t didx = acVertexBufferIdx(dst.x, dst.y, dst.z, device->local_config);
     const Layout& L   = device->L;
-    float* lo         = device->lo[device->cur] ? device->lo[device->cur] + h * L.fstride : nullptr;
+    float* lo         = device->lo[device->cur] ? device->lo[device->cur] + fidx(L, h, 0) : nullptr;
     device->ghost_ok[device->cur] = false;
     if (ensure_lo_ghosts(device, stream_of(device, stream), device->cur) != AC_SUCCESS)
         return AC_FAILURE;
     return copy_field_range(stream_of(device, stream), L,
-                            device->blk[device->cur] + h * L.fstride, didx,
+                            device->blk[device->cur] + fidx(L, h, 0), didx,
                             host_mesh.vertex_buffer[h] + sidx, (size_t)num_vertices, true, lo,
                             &device->stage);
 }
@@ -1139,9 +1115,9 @@ acDeviceStoreVertexBufferWithOffset(const Device device, const Stream stream,
     const size_t didx = acVertexBufferIdx(dst.x, dst.y, dst.z, host_mesh->info);
     const Layout& L   = device->L;
     return copy_field_range(stream_of(device, stream), L,
-                            device->blk[device->cur] + h * L.fstride, sidx,
+                            device->blk[device->cur] + fidx(L, h, 0), sidx,
                             host_mesh->vertex_buffer[h] + didx, (size_t)num_vertices, false,
-                            nullptr, nullptr);
+                            nullptr, &device->stage);
 }
 
 AcResult
@@ -1185,8 +1161,8 @@ transfer_kernel(const Layout Ls, const state_t* __restrict__ src, const float* _
          t += (long long)gridDim.x * blockDim.x) {
         const long long a = s0 + t, b = d0 + t;
         const long long ra = a / Ls.mx, rb = b / Ld.mx;
-        const long long ia = Ls.offx + ra * Ls.mxp + (a - ra * Ls.mx);
-        const long long ib = Ld.offx + rb * Ld.mxp + (b - rb * Ld.mx);
+        const long long ia = (Ls.offx + ra * Ls.mxp + (a - ra * Ls.mx)) * ACB_LANES;
+        const long long ib = (Ld.offx + rb * Ld.mxp + (b - rb * Ld.mx)) * ACB_LANES;
         dst[ib]            = src[ia];
         if (ACB_MIXED && dlo)
             dlo[ib] = slo ? slo[ia] : 0.f; // the (hi, lo) pair moves whole
@@ -1217,14 +1193,14 @@ acDeviceTransferVertexBufferWithOffset(const Device src_device, const Stream str
         ensure_lo_ghosts(dst_device, tst, dst_device->cur) != AC_SUCCESS)
         return AC_FAILURE;
     const float* slo = src_device->lo[src_device->cur]
-                           ? src_device->lo[src_device->cur] + h * src_device->L.fstride
+                           ? src_device->lo[src_device->cur] + fidx(src_device->L, h, 0)
                            : nullptr;
     float* dlo = dst_device->lo[dst_device->cur]
-                     ? dst_device->lo[dst_device->cur] + h * dst_device->L.fstride
+                     ? dst_device->lo[dst_device->cur] + fidx(dst_device->L, h, 0)
                      : nullptr;
     transfer_kernel<<<src_device->num_sms * 4, 256, 0, tst>>>(
-        src_device->L, src_device->blk[src_device->cur] + h * src_device->L.fstride, slo,
-        (long long)sidx, dst_device->L, dst_device->blk[dst_device->cur] + h * dst_device->L.fstride,
+        src_device->L, src_device->blk[src_device->cur] + fidx(src_device->L, h, 0), slo,
+        (long long)sidx, dst_device->L, dst_device->blk[dst_device->cur] + fidx(dst_device->L, h, 0),
         dlo, (long long)didx, (long long)num_vertices);
     ACB_CUDA_CHECK(cudaGetLastError());
     src_device->launches++;
@@ -1497,9 +1473,9 @@ acSolveConfigName(const int config)
 AcResult
 acDeviceGetMemoryFootprint(const Device device, size_t* bytes)
 {
-    size_t b = 2 * (size_t)device->L.fstride * ACB_NF * sizeof(state_t);
+    size_t b = 2 * block_bytes(device->L);
     if (device->lo[0])
-        b += 2 * (size_t)device->L.fstride * ACB_NF * sizeof(float);
+        b += 2 * block_bytes(device->L);
     *bytes = b;
     return AC_SUCCESS;
 }

@@ -359,13 +359,13 @@ acEnsembleCreate(const int device_id, const int num_members, const AcMeshInfo* c
             acEnsembleDestroy(e);
             return AC_FAILURE;
         }
-        mb.L               = make_layout(nx, ny, nz, (int)sizeof(state_t));
-        const size_t bytes = (size_t)mb.L.fstride * ACB_NF * sizeof(state_t);
+        mb.L               = make_layout(nx, ny, nz);
+        const size_t bytes = block_bytes(mb.L);
         for (int b = 0; b < 2; ++b) {
             ACB_CUDA_CHECK(cudaMalloc((void**)&mb.blk[b], bytes));
             ACB_CUDA_CHECK(cudaMemset(mb.blk[b], 0, bytes));
 #if ACB_MIXED
-            const size_t lb = (size_t)mb.L.fstride * ACB_NF * sizeof(float);
+            const size_t lb = block_bytes(mb.L);
             ACB_CUDA_CHECK(cudaMalloc((void**)&mb.lo[b], lb));
             ACB_CUDA_CHECK(cudaMemset(mb.lo[b], 0, lb));
 #endif
@@ -434,8 +434,8 @@ acEnsembleLoadMember(Ensemble e, const int member, const AcMesh host_mesh)
     }
     e->ghost_ok[e->cur] = false;
     for (int f = 0; f < NUM_VTXBUF_HANDLES; ++f) {
-        float* lo = mb.lo[e->cur] ? mb.lo[e->cur] + f * mb.L.fstride : nullptr;
-        if (copy_field_range(e->stream, mb.L, mb.blk[e->cur] + f * mb.L.fstride, 0,
+        float* lo = mb.lo[e->cur] ? mb.lo[e->cur] + fidx(mb.L, f, 0) : nullptr;
+        if (copy_field_range(e->stream, mb.L, mb.blk[e->cur] + fidx(mb.L, f, 0), 0,
                              host_mesh.vertex_buffer[f], n, true, lo, &e->stage) != AC_SUCCESS)
             return AC_FAILURE;
     }
@@ -456,8 +456,8 @@ acEnsembleStoreMember(Ensemble e, const int member, AcMesh* host_mesh)
         return AC_FAILURE;
     }
     for (int f = 0; f < NUM_VTXBUF_HANDLES; ++f)
-        if (copy_field_range(e->stream, mb.L, mb.blk[e->cur] + f * mb.L.fstride, 0,
-                             host_mesh->vertex_buffer[f], n, false, nullptr, nullptr) !=
+        if (copy_field_range(e->stream, mb.L, mb.blk[e->cur] + fidx(mb.L, f, 0), 0,
+                             host_mesh->vertex_buffer[f], n, false, nullptr, &e->stage) !=
             AC_SUCCESS)
             return AC_FAILURE;
     ACB_CUDA_CHECK(cudaStreamSynchronize(e->stream));

@@ -11,12 +11,15 @@
 // Whole-box fill (the case every integration step takes): the ghost vertices
 // split into two kinds of independent work units, all in one launch.
 //   A. interior rows (j, k both interior): only the 3 + 3 x-ghosts. One thread
-//      per (row, field) copies the six vertices of both halves (hi and lo in
-//      the mixed build): 6 or 12 independent loads before any store.
+//      per (row, array) copies the six elements of both sides: 6 independent
+//      loads before any store, or, with nx % 4 == 0, the two 32-byte sectors
+//      that hold the ghosts (with one padding element each) as whole sectors.
 //   B. ghost rows (j or k in the ghost zone): the whole row. One thread per
-//      (row, field, 128-vertex chunk, lane) copies four vertices 32 apart, so
-//      each warp instruction is one coalesced 128-byte row segment and each
-//      thread has 4 (8) loads in flight.
+//      (row, array, 128-element chunk, lane) copies four elements 32 apart, so
+//      each warp instruction is one coalesced 256-byte row segment and each
+//      thread has 4 loads in flight.
+// Both kinds move 8-byte elements of the block's arrays (a field pair, or one
+// double), whatever the fields.
 // A thread never stores before all its loads are issued, so memory-level
 // parallelism comes from the thread count, not from the warp count per row.
 // `lo` may be null: the mixed build's integration path fills the hi parts
@@ -30,7 +33,7 @@
 
 struct HaloArgs {
     Layout L;
-    state_t* block; // field block (in)
+    state_t* block; // block (in)
     float* lo;      // mixed build: lo block of `in` (else null)
     int3 start, end;
     int f0, f1; // fields [f0, f1)
@@ -54,15 +57,17 @@ halo_row(const Layout& L, state_t* block, float* lo, int3 start, int3 end, int f
     const int ks         = wrap_interior(k, L.nz);
     const long long drow = lidx(L, 0, j, k);
     const long long srow = lidx(L, 0, js, ks);
+    // field f's vertex id is at F[id * ACB_LANES], F = block + fidx(L, f, 0)
+    constexpr int W = ACB_LANES;
     if (ghost_row) {
         for (int f = f0; f < f1; ++f) {
-            state_t* F = block + f * L.fstride;
+            state_t* F = block + fidx(L, f, 0);
             for (int i = start.x + lane; i < end.x; i += 32)
-                F[drow + i] = F[srow + wrap_interior(i, L.nx)];
+                F[(drow + i) * W] = F[(srow + wrap_interior(i, L.nx)) * W];
             if (ACB_MIXED && lo) {
-                float* G = lo + f * L.fstride;
+                float* G = lo + fidx(L, f, 0);
                 for (int i = start.x + lane; i < end.x; i += 32)
-                    G[drow + i] = G[srow + wrap_interior(i, L.nx)];
+                    G[(drow + i) * W] = G[(srow + wrap_interior(i, L.nx)) * W];
             }
         }
     }
@@ -71,11 +76,11 @@ halo_row(const Layout& L, state_t* block, float* lo, int3 start, int3 end, int f
         if (i >= start.x && i < end.x) {
             const int is = wrap_interior(i, L.nx);
             for (int f = f0; f < f1; ++f) {
-                state_t* F = block + f * L.fstride;
-                F[drow + i] = F[srow + is];
+                state_t* F         = block + fidx(L, f, 0);
+                F[(drow + i) * W] = F[(srow + is) * W];
                 if (ACB_MIXED && lo) {
-                    float* G = lo + f * L.fstride;
-                    G[drow + i] = G[srow + is];
+                    float* G         = lo + fidx(L, f, 0);
+                    G[(drow + i) * W] = G[(srow + is) * W];
                 }
             }
         }
@@ -106,18 +111,18 @@ halo_chunks(const Layout& L)
     return (unsigned)(L.mx + 127) / 128;
 }
 
-// Work units of kind A (interior rows x fields) and A + B of one mesh.
+// Work units of kind A (interior rows x arrays) and A + B of one mesh.
 static inline long long
 halo_units_a(const Layout& L)
 {
-    return (long long)L.ny * L.nz * ACB_NF;
+    return (long long)L.ny * L.nz * ACB_NARR;
 }
 
 static inline long long
 halo_units(const Layout& L)
 {
     const long long ghost_rows = (long long)L.my * L.mz - (long long)L.ny * L.nz;
-    return halo_units_a(L) + ghost_rows * ACB_NF * halo_chunks(L) * 32;
+    return halo_units_a(L) + ghost_rows * ACB_NARR * halo_chunks(L) * 32;
 }
 
 // Periodic source of ghost-or-interior coordinate c in [0, n + 6), n >= NGHOST.
@@ -127,50 +132,45 @@ wrap_near(int c, int n)
     return c < NGHOST ? c + n : (c >= n + NGHOST ? c - n : c);
 }
 
+// The block's elements as 8-byte units (a field pair, or a double).
+typedef unsigned long long helem_t;
+
+// Kind A or B unit u of one block (hi parts, or the lo parts in the mixed
+// build: the same layout).
 __device__ __forceinline__ void
-halo_unit(const Layout& L, state_t* block, float* lo, unsigned units_a, unsigned u)
+halo_unit_block(const Layout& L, helem_t* block, unsigned units_a, unsigned u)
 {
     if (u < units_a) {
-        // kind A: x-ghosts of interior row r, field f
-        const unsigned f     = u % ACB_NF;
-        const unsigned r     = u / ACB_NF;
+        // kind A: x-ghosts of interior row r, array a
+        const unsigned ar    = u % ACB_NARR;
+        const unsigned r     = u / ACB_NARR;
         const unsigned kq    = r / (unsigned)L.ny;
         const int j          = NGHOST + (int)(r - kq * (unsigned)L.ny);
         const int k          = NGHOST + (int)kq;
-        const long long base = lidx(L, 0, j, k) + (long long)f * L.fstride;
-        state_t* F           = block + base;
-        if constexpr (sizeof(state_t) == 4) {
-            if ((L.nx & 3) == 0) {
-                // 4-byte elements (offx = 5), nx % 4 == 0: x = -1..2 and
-                // x = nx+3..nx+6 are aligned 16-byte groups of the row (x = -1
-                // and x = nx+6 are row padding, inside the row, and get their
-                // periodic images too); their sources x = nx-1..nx+2 and
-                // x = 3..6 are aligned groups as well. Group of x: (offx + x) / 4.
-                const int gl    = (L.offx - 1) >> 2;        // x = -1
-                const int gr    = (L.offx + L.nx + 3) >> 2; // x = nx + 3
-                const int sl    = (L.offx + L.nx - 1) >> 2; // x = nx - 1
-                const int sr    = (L.offx + 3) >> 2;        // x = 3
-                float4* R       = reinterpret_cast<float4*>(F - L.offx);
-                const float4 vl = R[sl];
-                const float4 vr = R[sr];
-                R[gl] = vl;
-                R[gr] = vr;
-#if ACB_MIXED
-                if (lo) {
-                    float4* G       = reinterpret_cast<float4*>(lo + base - L.offx);
-                    const float4 wl = G[sl];
-                    const float4 wr = G[sr];
-                    G[gl]           = wl;
-                    G[gr]           = wr;
-                }
-#endif
-                return;
-            }
+        helem_t* F           = block + (long long)ar * L.fstride + lidx(L, 0, j, k);
+        if ((L.nx & 3) == 0) {
+            // offx = 1, nx % 4 == 0: x = -1..2 and x = nx+3..nx+6 are whole
+            // 32-byte sectors of the row (x = -1 and x = nx+6 are row padding,
+            // inside the row, and get their periodic images too), and so are
+            // their sources x = nx-1..nx+2 and x = 3..6. Sector of x:
+            // (offx + x) / 4.
+            ulonglong2* R = reinterpret_cast<ulonglong2*>(F - L.offx);
+            const int gl  = 2 * ((L.offx - 1) >> 2);        // x = -1
+            const int gr  = 2 * ((L.offx + L.nx + 3) >> 2); // x = nx + 3
+            const int sl  = 2 * ((L.offx + L.nx - 1) >> 2); // x = nx - 1
+            const int sr  = 2 * ((L.offx + 3) >> 2);        // x = 3
+            const ulonglong2 l0 = R[sl], l1 = R[sl + 1];
+            const ulonglong2 r0 = R[sr], r1 = R[sr + 1];
+            R[gl]     = l0;
+            R[gl + 1] = l1;
+            R[gr]     = r0;
+            R[gr + 1] = r1;
+            return;
         }
-        state_t v[2 * NGHOST];
+        helem_t v[2 * NGHOST];
 #pragma unroll
         for (int q = 0; q < NGHOST; ++q) {
-            v[q]          = F[L.nx + q]; // source of ghost q is nx + q
+            v[q]          = F[L.nx + q];   // source of ghost q is nx + q
             v[NGHOST + q] = F[NGHOST + q]; // source of ghost nx + 3 + q is 3 + q
         }
 #pragma unroll
@@ -178,30 +178,14 @@ halo_unit(const Layout& L, state_t* block, float* lo, unsigned units_a, unsigned
             F[q]                 = v[q];
             F[L.nx + NGHOST + q] = v[NGHOST + q];
         }
-#if ACB_MIXED
-        if (lo) {
-            float* G = lo + base;
-            float w[2 * NGHOST];
-#pragma unroll
-            for (int q = 0; q < NGHOST; ++q) {
-                w[q]          = G[L.nx + q];
-                w[NGHOST + q] = G[NGHOST + q];
-            }
-#pragma unroll
-            for (int q = 0; q < NGHOST; ++q) {
-                G[q]                 = w[q];
-                G[L.nx + NGHOST + q] = w[NGHOST + q];
-            }
-        }
-#endif
         return;
     }
-    // kind B: 4 vertices, 32 apart, of a 128-vertex chunk of ghost row `row`
+    // kind B: 4 elements, 32 apart, of a 128-element chunk of ghost row `row`
     u -= units_a;
     const unsigned lane = u & 31;
     unsigned wq         = u >> 5;
-    const unsigned f    = wq % ACB_NF;
-    wq /= ACB_NF;
+    const unsigned ar   = wq % ACB_NARR;
+    wq /= ACB_NARR;
     const unsigned nch   = halo_chunks(L);
     const unsigned row   = wq / nch;
     const unsigned chunk = wq - row * nch;
@@ -215,22 +199,22 @@ halo_unit(const Layout& L, state_t* block, float* lo, unsigned units_a, unsigned
         k                 = kk < NGHOST ? (int)kk : L.nz + (int)kk;
     }
     else {
-        const unsigned r  = row - zrows;
-        const unsigned kk = r / (2 * NGHOST);
-        const unsigned jj = r - kk * (2 * NGHOST);
+        const unsigned rr = row - zrows;
+        const unsigned kk = rr / (2 * NGHOST);
+        const unsigned jj = rr - kk * (2 * NGHOST);
         k                 = NGHOST + (int)kk;
         j                 = jj < NGHOST ? (int)jj : L.ny + (int)jj;
     }
-    const long long fo = (long long)f * L.fstride;
-    const long long d  = fo + lidx(L, 0, j, k);
-    const long long s  = fo + lidx(L, 0, wrap_near(j, L.ny), wrap_near(k, L.nz));
+    const long long ao = (long long)ar * L.fstride;
+    const long long d  = ao + lidx(L, 0, j, k);
+    const long long sr = ao + lidx(L, 0, wrap_near(j, L.ny), wrap_near(k, L.nz));
     const int x0       = (int)(chunk * 128 + lane);
-    state_t v[4];
+    helem_t v[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int x = x0 + 32 * q;
         if (x < L.mx)
-            v[q] = block[s + wrap_near(x, L.nx)];
+            v[q] = block[sr + wrap_near(x, L.nx)];
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -238,23 +222,14 @@ halo_unit(const Layout& L, state_t* block, float* lo, unsigned units_a, unsigned
         if (x < L.mx)
             block[d + x] = v[q];
     }
-#if ACB_MIXED
-    if (lo) {
-        float w[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int x = x0 + 32 * q;
-            if (x < L.mx)
-                w[q] = lo[s + wrap_near(x, L.nx)];
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int x = x0 + 32 * q;
-            if (x < L.mx)
-                lo[d + x] = w[q];
-        }
-    }
-#endif
+}
+
+__device__ __forceinline__ void
+halo_unit(const Layout& L, void* block, void* lo, unsigned units_a, unsigned u)
+{
+    halo_unit_block(L, static_cast<helem_t*>(block), units_a, u);
+    if (lo)
+        halo_unit_block(L, static_cast<helem_t*>(lo), units_a, u);
 }
 
 static __global__ void __launch_bounds__(256)
@@ -329,12 +304,13 @@ mirror_kernel(const HaloArgs a, const float sign)
             if (!ghost_row && i >= NGHOST && i < NGHOST + L.nx)
                 continue; // interior vertex
             const int is = mirror_interior(i, L.nx);
+            constexpr int W = ACB_LANES;
             for (int f = a.f0; f < a.f1; ++f) {
-                state_t* F                         = a.block + f * L.fstride;
-                F[drow + i]                        = (state_t)sign * F[srow + is];
+                state_t* F        = a.block + fidx(L, f, 0);
+                F[(drow + i) * W] = (state_t)sign * F[(srow + is) * W];
                 if (ACB_MIXED && a.lo) {
-                    float* G    = a.lo + f * L.fstride;
-                    G[drow + i] = sign * G[srow + is];
+                    float* G          = a.lo + fidx(L, f, 0);
+                    G[(drow + i) * W] = sign * G[(srow + is) * W];
                 }
             }
         }

@@ -57,9 +57,11 @@ red_identity(int rtype)
 __device__ __forceinline__ double
 red_load(const ReduceArgs& a, int w, long long id)
 {
-    double v = (double)a.f[w][id];
+    // a.f[w] is the field's base in the block: its vertex id is ACB_LANES
+    // values further per element
+    double v = (double)a.f[w][id * ACB_LANES];
 #if ACB_MIXED
-    v += (double)a.lo[w][id];
+    v += (double)a.lo[w][id * ACB_LANES];
 #endif
     return v;
 }

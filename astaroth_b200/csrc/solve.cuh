@@ -114,7 +114,7 @@ struct CentreSet {
 };
 
 struct CentreMaps {
-    CUtensorMap m[3]; // (TX, TY, 1, 8) boxes over out hi, in lo, out lo
+    CUtensorMap m[3]; // (TX, TY, 1, arrays) boxes over out hi, in lo, out lo
 };
 
 template <int TX_, int TY_, int NP_, int MINB_, int NC_ = 0>
@@ -123,7 +123,7 @@ struct TileCfg {
     // NC > 0: the centre-only values of single-mesh single-precision substeps
     // arrive by TMA in a ring of NC output-plane slots (else plain loads)
     static constexpr int NC = NC_;
-    static constexpr int CENTRE = TX_ * TY_ * ACB_NF; // elements of one centre array
+    static constexpr int CENTRE = TX_ * TY_ * ACB_NARR; // elements of one centre array set
     static constexpr int BX = TX_ + 8, BY = TY_ + 6;
     static constexpr int CONSUMERS = TX_ * TY_;        // one thread per (x, y) column
     static constexpr int CWARPS    = CONSUMERS / 32;   // consumer warps
@@ -138,12 +138,12 @@ struct TileCfg {
     // registers a thread the launch must hold for the reallocation to balance
     static constexpr int REG_LAUNCH =
         WGSPEC ? (REG_CONSUMER * CONSUMERS + REG_PRODUCER * 128 + THREADS - 1) / THREADS : 0;
-    static constexpr int FIELD   = BX * BY;
-    static constexpr int PLANE   = ACB_NF * FIELD; // elements per ring slot
-    static constexpr size_t ring_bytes() { return (size_t)NP * PLANE * sizeof(state_t); }
+    static constexpr int FIELD   = BX * BY;           // elements per array of a ring slot
+    static constexpr int PLANE   = ACB_NARR * FIELD;  // elements per ring slot
+    static constexpr size_t ring_bytes() { return (size_t)NP * PLANE * ACB_ELEM; }
     static constexpr size_t centre_slot_bytes()
     {
-        return (size_t)(ACB_MIXED ? 3 : 1) * CENTRE * sizeof(float);
+        return (size_t)(ACB_MIXED ? 3 : 1) * CENTRE * ACB_ELEM;
     }
     static constexpr size_t smem_bytes() { return ring_bytes() + NC * centre_slot_bytes(); }
 };
@@ -271,88 +271,12 @@ field_derivs(const state_t* __restrict__ c, const int* zo, const SolveParams<T>&
     return r;
 }
 
-// Register queue of one field along z (2.5D streaming): the values of the
-// thread's own column at the three planes below the current one, and, for a
-// field with an xz (yz) cross derivative, the lower half of that derivative
-// as running sums. The diagonal cross derivative at plane z,
-//   sum_k e_k (f(+k,+k) + f(-k,-k) - f(+k,-k) - f(-k,+k))
-//     = U(z) - L(z),  U(z) = sum_k e_k d_k(z+k),  L(z) = sum_k e_k d_k(z-k),
-// with d_k(w) = f(+k) - f(-k) the x (y) difference at plane w: the differences
-// of the current plane are formed for the first derivative anyway, and each
-// contributes e_k d_k(z) to L(z+k). So the queue keeps
-//   a1 = L(z),  a2 = the part of L(z+1) known so far,  a3 = that of L(z+2),
-// and advancing a plane is three fused multiply-adds (no register moves):
-//   a1 <- e1 d1(z) + a2,  a2 <- e2 d2(z) + a3,  a3 <- e3 d3(z).
-// Only the upper half U is read from the ring.
-template <typename T>
-struct ZQueue {
-    T v1, v2, v3;    // f at z-1, z-2, z-3
-    T xa1, xa2, xa3; // xz lower half: L(z), partial L(z+1), partial L(z+2)
-    T ya1, ya2, ya3; // the same for yz
-};
-
-__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
-
-// Advances the lower-half sums of one z diagonal past the plane whose
-// differences are d1, d2, d3 (e: the diagonal's coefficients). The rounding
-// sequence is fixed (explicit fma / mul), so prime_queue below reproduces the
-// sums a streaming task would have built, bit for bit.
-__device__ __forceinline__ void
-zacc_push(float& a1, float& a2, float& a3, const float* e, float d1, float d2, float d3)
-{
-    a1 = fma_rn(e[0], d1, a2);
-    a2 = fma_rn(e[1], d2, a3);
-    a3 = mul_rn(e[2], d3);
-}
-
-// Lower-half sums of one z diagonal at the first plane of a task from the
-// three planes below it (zo[0..2]); step: 1 for xz, the row pitch for yz.
-__device__ __forceinline__ void
-zacc_prime(const float* __restrict__ c, const int* zo, int step, const float* e, float& a1,
-           float& a2, float& a3)
-{
-    auto d = [&](int plane, int k) { return c[zo[plane] + k * step] - c[zo[plane] - k * step]; };
-    // plane z-3: only its third difference reaches L(z)
-    const float t3 = mul_rn(e[2], d(0, 3));
-    // plane z-2
-    const float b2 = fma_rn(e[1], d(1, 2), t3);
-    const float b3 = mul_rn(e[2], d(1, 3));
-    // plane z-1
-    a1 = fma_rn(e[0], d(2, 1), b2);
-    a2 = fma_rn(e[1], d(2, 2), b3);
-    a3 = mul_rn(e[2], d(2, 3));
-}
-
-// Upper half U of one z diagonal (u1..u3: d_k at plane z+k), in the order
-// every caller uses.
-__device__ __forceinline__ float
-zacc_upper(const float* e, float u1, float u2, float u3)
-{
-    return fma_rn(e[2], u3, fma_rn(e[1], u2, mul_rn(e[0], u1)));
-}
-
-// Fills the queue from the ring at the first plane of a task (zo[0..2]: the
-// three planes below it).
-template <int BX, bool XZ, bool YZ>
-__device__ __forceinline__ void
-prime_queue(const float* __restrict__ c, const int* zo, const SolveParams<float>& P,
-            ZQueue<float>& Q)
-{
-    Q.v1 = c[zo[2]];
-    Q.v2 = c[zo[1]];
-    Q.v3 = c[zo[0]];
-    if (XZ)
-        zacc_prime(c, zo, 1, P.cx[1], Q.xa1, Q.xa2, Q.xa3);
-    if (YZ)
-        zacc_prime(c, zo, BX, P.cx[2], Q.ya1, Q.ya2, Q.ya3);
-}
-
 // ---- pairs of fields in packed FP32 lanes ----------------------------------
-// add/sub.rn.f32x2 operate on two independent FP32 lanes with the rounding of
-// the scalar operations, so a pair of fields whose stencils have the same
-// shape forms its sums and differences in half the instructions, bit for bit
-// as one field at a time.
+// add/sub/mul/fma.rn.f32x2 operate on two independent FP32 lanes with the
+// rounding of the scalar operations, so a pair of fields whose stencils have
+// the same shape forms its sums and differences in half the instructions, bit
+// for bit as one field at a time. In the single-precision layout a pair is one
+// array of 8-byte (A, B) elements, so an F2 is also one 8-byte load.
 struct F2 {
     unsigned long long v;
 };
@@ -403,59 +327,126 @@ fma2(F2 a, F2 b, F2 c)
     return r;
 }
 
+// Register queue of one field along z (2.5D streaming): the values of the
+// thread's own column at the three planes below the current one and, for a
+// field with an xz (yz) cross derivative, the lower half of that derivative
+// as running sums. The diagonal cross derivative at plane z,
+//   sum_k e_k (f(+k,+k) + f(-k,-k) - f(+k,-k) - f(-k,+k))
+//     = U(z) - L(z),  U(z) = sum_k e_k d_k(z+k),  L(z) = sum_k e_k d_k(z-k),
+// with d_k(w) = f(+k) - f(-k) the x (y) difference at plane w: the differences
+// of the current plane are formed for the first derivative anyway, and each
+// contributes e_k d_k(z) to L(z+k). So the queue keeps
+//   a1 = L(z),  a2 = the part of L(z+1) known so far,  a3 = that of L(z+2),
+// and advancing a plane is three fused multiply-adds (no register moves):
+//   a1 <- e1 d1(z) + a2,  a2 <- e2 d2(z) + a3,  a3 <- e3 d3(z).
+// Only the upper half U is read from the ring.
+template <typename T>
+struct ZQueue {
+    T v1, v2, v3;    // f at z-1, z-2, z-3
+    T xa1, xa2, xa3; // xz lower half: L(z), partial L(z+1), partial L(z+2)
+    T ya1, ya2, ya3; // the same for yz
+};
+
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+
+// Advances the lower-half sums of one z diagonal past the plane whose
+// differences are d1, d2, d3 (e: the diagonal's coefficients). The rounding
+// sequence is fixed (explicit fma / mul), so prime_pair below reproduces the
+// sums a streaming task would have built, bit for bit.
+__device__ __forceinline__ void
+zacc_push(float& a1, float& a2, float& a3, const float* e, float d1, float d2, float d3)
+{
+    a1 = fma_rn(e[0], d1, a2);
+    a2 = fma_rn(e[1], d2, a3);
+    a3 = mul_rn(e[2], d3);
+}
+
+// Upper half U of one z diagonal (u1..u3: d_k at plane z+k), in the order
+// every caller uses.
+__device__ __forceinline__ float
+zacc_upper(const float* e, float u1, float u2, float u3)
+{
+    return fma_rn(e[2], u3, fma_rn(e[1], u2, mul_rn(e[0], u1)));
+}
+
+// Lower-half sums of the z diagonals of both fields of a pair at the first
+// plane of a task from the three planes below it (zo[0..2]); step: 1 for xz,
+// the row pitch for yz. The differences are formed in packed lanes, as the
+// streaming plane forms them.
+__device__ __forceinline__ void
+zacc_prime2(const F2* __restrict__ c, const int* zo, int step, const float* e, float (&A)[3],
+            float (&B)[3])
+{
+    float dA[3][4], dB[3][4]; // [plane z-3 + p][k]
+#pragma unroll
+    for (int p = 0; p < 3; ++p)
+#pragma unroll
+        for (int k = 1; k <= 3; ++k)
+            upk2(sub2(c[zo[p] + k * step], c[zo[p] - k * step]), dA[p][k], dB[p][k]);
+    auto prime = [&](const float (&d)[3][4], float (&a)[3]) {
+        // plane z-3: only its third difference reaches L(z)
+        const float t3 = mul_rn(e[2], d[0][3]);
+        // plane z-2
+        const float b2 = fma_rn(e[1], d[1][2], t3);
+        const float b3 = mul_rn(e[2], d[1][3]);
+        // plane z-1
+        a[0] = fma_rn(e[0], d[2][1], b2);
+        a[1] = fma_rn(e[1], d[2][2], b3);
+        a[2] = mul_rn(e[2], d[2][3]);
+    };
+    prime(dA, A);
+    prime(dB, B);
+}
+
+// Fills the queues of the fields of one pair array c from the ring at the
+// first plane of a task (zo[0..2]: the three planes below it). Both fields of
+// a pair have the same z diagonals (XZ, YZ).
+template <int BX, bool XZ, bool YZ>
+__device__ __forceinline__ void
+prime_pair(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P, ZQueue<float>& QA,
+           ZQueue<float>& QB)
+{
+    upk2(c[zo[2]], QA.v1, QB.v1);
+    upk2(c[zo[1]], QA.v2, QB.v2);
+    upk2(c[zo[0]], QA.v3, QB.v3);
+    if (XZ) {
+        float A[3], B[3];
+        zacc_prime2(c, zo, 1, P.cx[1], A, B);
+        QA.xa1 = A[0], QA.xa2 = A[1], QA.xa3 = A[2];
+        QB.xa1 = B[0], QB.xa2 = B[1], QB.xa3 = B[2];
+    }
+    if (YZ) {
+        float A[3], B[3];
+        zacc_prime2(c, zo, BX, P.cx[2], A, B);
+        QA.ya1 = A[0], QA.ya2 = A[1], QA.ya3 = A[2];
+        QB.ya1 = B[0], QB.ya2 = B[1], QB.ya3 = B[2];
+    }
+}
+
 template <bool GX_, bool GY_, bool GZ_, bool XY_, bool XZ_, bool YZ_>
 struct DFlags {
     static constexpr bool GX = GX_, GY = GY_, GZ = GZ_, XY = XY_, XZ = XZ_, YZ = YZ_;
 };
 
-// A z-diagonal cross derivative (XK: xz, else yz) of one lane: the ring step
-// of its points, its coefficients and its queued lower half.
+// The z-diagonal cross derivative of kind XK (xz, else yz) of both fields of
+// a pair: the upper-half differences in packed lanes (one 8-byte load per
+// point), the coefficient sums and the queued lower halves per field.
 template <bool XK, int BX>
-struct ZCross {
-    static constexpr int step = XK ? 1 : BX;
-    static constexpr int row  = XK ? 1 : 2;
-    __device__ __forceinline__ static float lower(const ZQueue<float>& Q)
-    {
-        return XK ? Q.xa1 : Q.ya1;
-    }
-};
-
-// Two z-diagonal cross derivatives (one of field A, kind XA; one of field B,
-// kind XB) with the upper-half differences formed in packed lanes.
-template <bool XA, bool XB, int BX>
 __device__ __forceinline__ void
-zcross_pair(const float* __restrict__ cA, const float* __restrict__ cB, const int* zo,
-            const SolveParams<float>& P, const ZQueue<float>& QA, const ZQueue<float>& QB,
-            float& sA, float& sB)
+zcross_pair(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P,
+            const ZQueue<float>& QA, const ZQueue<float>& QB, float& sA, float& sB)
 {
-    using CA = ZCross<XA, BX>;
-    using CB = ZCross<XB, BX>;
+    constexpr int step = XK ? 1 : BX;
+    const float* e     = P.cx[XK ? 1 : 2];
     float a[3], b[3];
 #pragma unroll
     for (int k = 1; k <= 3; ++k) {
         const int z = zo[3 + k];
-        const F2 u  = sub2(pk2(cA[z + k * CA::step], cB[z + k * CB::step]),
-                           pk2(cA[z - k * CA::step], cB[z - k * CB::step]));
-        upk2(u, a[k - 1], b[k - 1]);
+        upk2(sub2(c[z + k * step], c[z - k * step]), a[k - 1], b[k - 1]);
     }
-    sA = zacc_upper(P.cx[CA::row], a[0], a[1], a[2]) - CA::lower(QA);
-    sB = zacc_upper(P.cx[CB::row], b[0], b[1], b[2]) - CB::lower(QB);
-}
-
-// One z-diagonal cross derivative of one field (no partner).
-template <bool XK, int BX>
-__device__ __forceinline__ float
-zcross_one(const float* __restrict__ c, const int* zo, const SolveParams<float>& P,
-           const ZQueue<float>& Q)
-{
-    using CK = ZCross<XK, BX>;
-    float u[3];
-#pragma unroll
-    for (int k = 1; k <= 3; ++k) {
-        const int z = zo[3 + k];
-        u[k - 1]    = c[z + k * CK::step] - c[z - k * CK::step];
-    }
-    return zacc_upper(P.cx[CK::row], u[0], u[1], u[2]) - CK::lower(Q);
+    sA = zacc_upper(e, a[0], a[1], a[2]) - (XK ? QA.xa1 : QA.ya1);
+    sB = zacc_upper(e, b[0], b[1], b[2]) - (XK ? QB.xa1 : QB.ya1);
 }
 
 // Advances a queue by one plane (after every use of it): f0 and the x / y
@@ -474,26 +465,29 @@ push_queue(ZQueue<float>& Q, const SolveParams<float>& P, float f0, const float*
     Q.v1 = f0;
 }
 
-// The derivatives of two fields at once: every
-// pencil sum and difference, the xy diagonals both fields need and the paired
-// z diagonals in packed lanes; the coefficient sums per field. Second
-// derivatives in difference form (below).
+// The derivatives of the two fields of one pair array c at once: every pencil
+// sum and difference, the xy diagonals and the z diagonals in packed lanes
+// (each stencil point one 8-byte load); the coefficient sums. Second
+// derivatives in difference form (below). F0 returns the pair's centre values.
 template <int BX, class FA, class FB>
 __device__ __forceinline__ void
-pair_derivs_q(const float* __restrict__ cA, const float* __restrict__ cB, const int* zo,
-              const SolveParams<float>& P, ZQueue<float>& QA, ZQueue<float>& QB,
-              FieldDerivs<float>& rA, FieldDerivs<float>& rB)
+pair_derivs_q(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P,
+              ZQueue<float>& QA, ZQueue<float>& QB, FieldDerivs<float>& rA,
+              FieldDerivs<float>& rB, F2& F0)
 {
-    const float a0 = cA[0], b0 = cB[0];
-    rA.v        = a0;
-    rB.v        = b0;
-    const F2 F0 = pk2(a0, b0);
+    static_assert(FA::XY == FB::XY && FA::XZ == FB::XZ && FA::YZ == FB::YZ,
+                  "the fields of a pair have the same cross derivatives");
+    F0 = c[0];
+    float a0, b0;
+    upk2(F0, a0, b0);
+    rA.v = a0;
+    rB.v = b0;
     F2 DX[3], SX[3], DY[3], SY[3], DZ[3], SZ[3];
     // Second differences as u + v with u = f(+k) - f0, v = f(-k) - f0: for a
     // smooth field u and v are exact in FP32 (Sterbenz), so f(+k) + f(-k) - 2 f0
     // keeps its digits instead of cancelling terms of size |c0 f0| (about
     // 2.7 f / ds^2); mathematically the same stencil (c0 = -2 (c1 + c2 + c3)).
-    // First differences f(+k) - f(-k) directly, as prime_queue forms the queued
+    // First differences f(+k) - f(-k) directly, as prime_pair forms the queued
     // ones, so results do not depend on where a task's z segment starts.
     auto dsum = [&](F2 p, F2 m, F2& D, F2& S) {
         D = sub2(p, m);
@@ -501,18 +495,18 @@ pair_derivs_q(const float* __restrict__ cA, const float* __restrict__ cB, const 
     };
 #pragma unroll
     for (int k = 1; k <= 3; ++k) {
-        dsum(pk2(cA[k], cB[k]), pk2(cA[-k], cB[-k]), DX[k - 1], SX[k - 1]);
-        dsum(pk2(cA[k * BX], cB[k * BX]), pk2(cA[-k * BX], cB[-k * BX]), DY[k - 1], SY[k - 1]);
+        dsum(c[k], c[-k], DX[k - 1], SX[k - 1]);
+        dsum(c[k * BX], c[-k * BX], DY[k - 1], SY[k - 1]);
     }
-    dsum(pk2(cA[zo[4]], cB[zo[4]]), pk2(QA.v1, QB.v1), DZ[0], SZ[0]);
-    dsum(pk2(cA[zo[5]], cB[zo[5]]), pk2(QA.v2, QB.v2), DZ[1], SZ[1]);
-    dsum(pk2(cA[zo[6]], cB[zo[6]]), pk2(QA.v3, QB.v3), DZ[2], SZ[2]);
+    dsum(c[zo[4]], pk2(QA.v1, QB.v1), DZ[0], SZ[0]);
+    dsum(c[zo[5]], pk2(QA.v2, QB.v2), DZ[1], SZ[1]);
+    dsum(c[zo[6]], pk2(QA.v3, QB.v3), DZ[2], SZ[2]);
     // Coefficient sums sum_k c_k d_k of both fields. The FP32 build forms them
     // in packed lanes ((c, c) coefficient pairs; 2-3 % faster per step at
     // 512^3); the mixed build, whose update holds more registers, runs 2 %
     // faster with them in scalar form (the same operations per lane).
     constexpr bool PACKED_SUMS = !ACB_MIXED;
-    auto sum3 = [&](const unsigned long long* cp, const float* c, const F2* d, float& oa,
+    auto sum3 = [&](const unsigned long long* cp, const float* cs, const F2* d, float& oa,
                     float& ob) {
         if constexpr (PACKED_SUMS) {
             F2 r = mul2(F2{cp[0]}, d[0]);
@@ -524,8 +518,8 @@ pair_derivs_q(const float* __restrict__ cA, const float* __restrict__ cB, const 
 #pragma unroll
             for (int k = 0; k < 3; ++k)
                 upk2(d[k], a[k], b[k]);
-            oa = c[0] * a[0] + c[1] * a[1] + c[2] * a[2];
-            ob = c[0] * b[0] + c[1] * b[1] + c[2] * b[2];
+            oa = cs[0] * a[0] + cs[1] * a[1] + cs[2] * a[2];
+            ob = cs[0] * b[0] + cs[1] * b[1] + cs[2] * b[2];
         }
     };
     float gA, gB;
@@ -556,40 +550,21 @@ pair_derivs_q(const float* __restrict__ cA, const float* __restrict__ cB, const 
     }
 
     // xy diagonals (the whole stencil from the centre plane)
-    if (FA::XY || FB::XY) {
-        static_assert(FA::XY == FB::XY, "xy diagonals are formed for both fields of a pair");
+    if (FA::XY) {
         F2 E[3];
 #pragma unroll
         for (int k = 1; k <= 3; ++k) {
             const int pp = k + k * BX, mm = -k - k * BX, pm = k - k * BX, mp = -k + k * BX;
-            const F2 a = add2(pk2(cA[pp], cB[pp]), pk2(cA[mm], cB[mm]));
-            const F2 b = add2(pk2(cA[pm], cB[pm]), pk2(cA[mp], cB[mp]));
-            E[k - 1]   = sub2(a, b);
+            E[k - 1] = sub2(add2(c[pp], c[mm]), add2(c[pm], c[mp]));
         }
         sum3(P.cxp, P.cx[0], E, rA.xy, rB.xy);
     }
 
-    // z diagonals: the first of A's with the first of B's, the second with the second
-    constexpr int nA = (FA::XZ ? 1 : 0) + (FA::YZ ? 1 : 0);
-    constexpr int nB = (FB::XZ ? 1 : 0) + (FB::YZ ? 1 : 0);
-    constexpr bool A1X = FA::XZ, B1X = FB::XZ; // kind of each field's first z diagonal
-    float zA[2] = {0, 0}, zB[2] = {0, 0};
-    if constexpr (nA >= 1 && nB >= 1)
-        zcross_pair<A1X, B1X, BX>(cA, cB, zo, P, QA, QB, zA[0], zB[0]);
-    else if constexpr (nA >= 1)
-        zA[0] = zcross_one<A1X, BX>(cA, zo, P, QA);
-    else if constexpr (nB >= 1)
-        zB[0] = zcross_one<B1X, BX>(cB, zo, P, QB);
-    if constexpr (nA == 2 && nB == 2)
-        zcross_pair<false, false, BX>(cA, cB, zo, P, QA, QB, zA[1], zB[1]);
-    else if constexpr (nA == 2)
-        zA[1] = zcross_one<false, BX>(cA, zo, P, QA);
-    else if constexpr (nB == 2)
-        zB[1] = zcross_one<false, BX>(cB, zo, P, QB);
-    if (FA::XZ) rA.xz = zA[0];
-    if (FA::YZ) rA.yz = FA::XZ ? zA[1] : zA[0];
-    if (FB::XZ) rB.xz = zB[0];
-    if (FB::YZ) rB.yz = FB::XZ ? zB[1] : zB[0];
+    // z diagonals (both fields have the same kinds)
+    if (FA::XZ)
+        zcross_pair<true, BX>(c, zo, P, QA, QB, rA.xz, rB.xz);
+    if (FA::YZ)
+        zcross_pair<false, BX>(c, zo, P, QA, QB, rA.yz, rB.yz);
 
     push_queue<FA::XZ, FA::YZ>(QA, P, a0, dxA, dyA);
     push_queue<FB::XZ, FB::YZ>(QB, P, b0, dxB, dyB);
@@ -631,38 +606,35 @@ mhd_rhs(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, T
     rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
 }
 
-// The same with the z register queues (single-precision stencils), in pairs
-// of like-shaped stencils, two packed lanes per instruction.
+// The same with the z register queues (single-precision stencils), one pair
+// array at a time: (lnrho, ss), (ux, ax), (uy, ay), (uz, az). cur2 returns the
+// centre values of each array.
 template <int BX, int FIELD>
 __device__ __forceinline__ void
-mhd_rhs_q(const float* __restrict__ c, const int* zo, const SolveParams<float>& P,
-          float roc[ACB_NF], float cur[ACB_NF], ZQueue<float> (&Q)[ACB_NF])
+mhd_rhs_q(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P,
+          float roc[ACB_NF], float cur[ACB_NF], F2 cur2[ACB_NARR], ZQueue<float> (&Q)[ACB_NF])
 {
     FieldDerivs<float> lr, ux, uy, uz, ax, ay, az, ss;
-    pair_derivs_q<BX, DFlags<ACB_D_LNRHO>, DFlags<ACB_D_SS>>(c + 0 * FIELD, c + 7 * FIELD, zo, P,
-                                                             Q[0], Q[7], lr, ss);
-    pair_derivs_q<BX, DFlags<ACB_D_UUX>, DFlags<ACB_D_UUY>>(c + 1 * FIELD, c + 2 * FIELD, zo, P,
-                                                            Q[1], Q[2], ux, uy);
-    pair_derivs_q<BX, DFlags<ACB_D_AX>, DFlags<ACB_D_AY>>(c + 4 * FIELD, c + 5 * FIELD, zo, P,
-                                                          Q[4], Q[5], ax, ay);
-    pair_derivs_q<BX, DFlags<ACB_D_UUZ>, DFlags<ACB_D_AZ>>(c + 3 * FIELD, c + 6 * FIELD, zo, P,
-                                                           Q[3], Q[6], uz, az);
+    pair_derivs_q<BX, DFlags<ACB_D_LNRHO>, DFlags<ACB_D_SS>>(c + 0 * FIELD, zo, P, Q[0], Q[7], lr,
+                                                             ss, cur2[0]);
+    pair_derivs_q<BX, DFlags<ACB_D_UUX>, DFlags<ACB_D_AX>>(c + 1 * FIELD, zo, P, Q[1], Q[4], ux,
+                                                           ax, cur2[1]);
+    pair_derivs_q<BX, DFlags<ACB_D_UUY>, DFlags<ACB_D_AY>>(c + 2 * FIELD, zo, P, Q[2], Q[5], uy,
+                                                           ay, cur2[2]);
+    pair_derivs_q<BX, DFlags<ACB_D_UUZ>, DFlags<ACB_D_AZ>>(c + 3 * FIELD, zo, P, Q[3], Q[6], uz,
+                                                           az, cur2[3]);
     rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
 }
 
 template <int BX, int FIELD>
 __device__ __forceinline__ void
-prime_queues(const float* __restrict__ c, const int* zo, const SolveParams<float>& P,
+prime_queues(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P,
              ZQueue<float> (&Q)[ACB_NF])
 {
-    prime_queue<BX, false, false>(c + 0 * FIELD, zo, P, Q[0]);
-    prime_queue<BX, true, false>(c + 1 * FIELD, zo, P, Q[1]);
-    prime_queue<BX, false, true>(c + 2 * FIELD, zo, P, Q[2]);
-    prime_queue<BX, true, true>(c + 3 * FIELD, zo, P, Q[3]);
-    prime_queue<BX, true, false>(c + 4 * FIELD, zo, P, Q[4]);
-    prime_queue<BX, false, true>(c + 5 * FIELD, zo, P, Q[5]);
-    prime_queue<BX, true, true>(c + 6 * FIELD, zo, P, Q[6]);
-    prime_queue<BX, false, false>(c + 7 * FIELD, zo, P, Q[7]);
+    prime_pair<BX, false, false>(c + 0 * FIELD, zo, P, Q[0], Q[7]);
+    prime_pair<BX, true, false>(c + 1 * FIELD, zo, P, Q[1], Q[4]);
+    prime_pair<BX, false, true>(c + 2 * FIELD, zo, P, Q[2], Q[5]);
+    prime_pair<BX, true, true>(c + 3 * FIELD, zo, P, Q[3], Q[6]);
 }
 
 // Right-hand sides from the derivative sets (stencil_kernel.ac:355-528,
@@ -822,25 +794,45 @@ pair_add2(F2 hi, F2 lo, F2 d, F2& ohi, F2& olo)
 
 // Values of the vertex's own column that the update needs besides the ring:
 // the previous state (s > 0) and, in the mixed build, the lo parts.
+// FP64 build: one value per field.
 struct CentreVals {
     AcReal prev[ACB_NF];
-    float cur_lo[ACB_NF];
-    float prev_lo[ACB_NF];
 };
 
 template <int STEP>
 __device__ __forceinline__ void
-load_centre(const Layout& L, const state_t* out, const float* in_lo, const float* out_lo,
-            long long id, CentreVals& c)
+load_centre(const Layout& L, const state_t* out, long long id, CentreVals& c)
 {
-    const long long fs = L.fstride;
 #pragma unroll
-    for (int f = 0; f < ACB_NF; ++f) {
+    for (int f = 0; f < ACB_NF; ++f)
         if (STEP > 0)
-            c.prev[f] = out[f * fs + id];
+            c.prev[f] = out[fidx(L, f, id)];
+}
+
+// Single-precision layout: one (A, B) element per pair array; lo parts in
+// the mixed build.
+struct CentreVals2 {
+    acb::F2 prev[ACB_NARR];
+    acb::F2 cur_lo[ACB_NARR];
+    acb::F2 prev_lo[ACB_NARR];
+};
+
+template <int STEP>
+__device__ __forceinline__ void
+load_centre2(const Layout& L, const state_t* out, const float* in_lo, const float* out_lo,
+             long long id, CentreVals2& c)
+{
+    const acb::F2* o  = reinterpret_cast<const acb::F2*>(out);
+    const acb::F2* il = reinterpret_cast<const acb::F2*>(in_lo);
+    const acb::F2* ol = reinterpret_cast<const acb::F2*>(out_lo);
+#pragma unroll
+    for (int a = 0; a < ACB_NARR; ++a) {
+        const long long e = a * L.fstride + id;
+        if (STEP > 0)
+            c.prev[a] = o[e];
 #if ACB_MIXED
-        c.cur_lo[f]  = in_lo[f * fs + id];
-        c.prev_lo[f] = STEP > 0 ? out_lo[f * fs + id] : 0.f;
+        c.cur_lo[a]  = il[e];
+        c.prev_lo[a] = STEP > 0 ? ol[e] : acb::F2{0ull};
 #endif
     }
 }
@@ -892,9 +884,9 @@ member_of(const MemberDesc<T>* md, int n, long long t)
 template <class Cfg, int STEP, bool ENS>
 __device__ __forceinline__ bool
 consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<AcReal>& P,
-             long long lt, state_t* out, float* in_lo, float* out_lo, const state_t* ring,
+             long long lt, state_t* out, float* in_lo, float* out_lo, const void* ring,
              uint64_t* full, uint64_t* empty, volatile int* abort_flag, uint32_t& q,
-             const float* centre, uint64_t* full_c, uint64_t* empty_c, uint32_t& oq)
+             const void* centre, uint64_t* full_c, uint64_t* empty_c, uint32_t& oq)
 {
     using CS          = CentreSet<STEP>;
     constexpr bool CT = Cfg::NC > 0 && !ENS && CS::STAGE;
@@ -912,16 +904,18 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
     const int j     = tg.j0 + ty;
     const bool act  = (i >= gv.start.x) && (i < gv.end.x) && (j < gv.end.y);
     const T rkA     = a.P.rkA, rkB = a.P.rkB;
+    // this thread's column in a ring slot (elements)
+    const int col = (ty + NGHOST) * BX + (tx + 4);
 
     bool ok = true;
     for (int l = 0; l < 2 * NGHOST && ok; ++l)
         ok = mbar_wait_bounded(&full[(q + l) % NP], ((q + l) / NP) & 1u);
     ok = __all_sync(0xffffffffu, ok);
 
-    // single precision streams with the z register queues (2.5D); double
-    // precision has no registers to spare for them and reads every operand
-    // from the ring
-    constexpr bool QZ = sizeof(state_t) == 4;
+    // single precision streams with the z register queues (2.5D) over the pair
+    // arrays; double precision has no registers to spare for them and reads
+    // every operand from the ring
+    constexpr bool QZ = ACB_PAIRED;
     acb::ZQueue<float> Q[ACB_NF];
     if constexpr (QZ) {
         if (ok && act) {
@@ -930,7 +924,7 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
 #pragma unroll
             for (int dz = -NGHOST; dz <= NGHOST; ++dz)
                 zo[dz + NGHOST] = ((int)((q + NGHOST + dz) % NP) - (int)sc) * PLANE;
-            const state_t* c = ring + (size_t)sc * PLANE + (ty + NGHOST) * BX + (tx + 4);
+            const acb::F2* c = reinterpret_cast<const acb::F2*>(ring) + (size_t)sc * PLANE + col;
             acb::prime_queues<BX, FIELD>(c, zo, P, Q);
         }
         // the three planes below the first output plane now live in the queues
@@ -944,8 +938,9 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
     // values of the next plane are loaded a plane ahead
     constexpr bool PREF = !QZ;
     CentreVals cv_next;
-    if (PREF && act)
-        load_centre<STEP>(L, out, in_lo, out_lo, lidx(L, i, j, tg.k0), cv_next);
+    if constexpr (PREF)
+        if (act)
+            load_centre<STEP>(L, out, lidx(L, i, j, tg.k0), cv_next);
 
     for (int p = 0; p < tg.nout; ++p) {
         if (ok) {
@@ -969,23 +964,7 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
         const int k = tg.k0 + p;
         if (act) {
             const long long id = lidx(L, i, j, k);
-            // previous state and lo parts of this vertex: issued first, used
-            // only by the update at the end of the plane
-            CentreVals cv;
-            if constexpr (PREF) {
-                cv = cv_next;
-                if (p + 1 < tg.nout)
-                    load_centre<STEP>(L, out, in_lo, out_lo, id + L.plane, cv_next);
-            }
-            else if constexpr (CT) {
-                // read from the centre slot after the right-hand sides (below):
-                // the values are in shared memory already, and reading them
-                // late keeps 24 registers free through the stencils
-            }
-            else {
-                load_centre<STEP>(L, out, in_lo, out_lo, id, cv);
-            }
-            const uint32_t sc = (q + p + NGHOST) % NP;
+            const uint32_t sc  = (q + p + NGHOST) % NP;
             int zo[7];
 #pragma unroll
             for (int dz = -NGHOST; dz <= NGHOST; ++dz) {
@@ -994,89 +973,106 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
                 const int sd    = (int)((q + p + NGHOST + dz) % NP);
                 zo[dz + NGHOST] = (sd - (int)sc) * PLANE;
             }
-            const state_t* c = ring + (size_t)sc * PLANE + (ty + NGHOST) * BX + (tx + 4);
-
-            T roc[ACB_NF], cur[ACB_NF];
-            if constexpr (QZ)
-                acb::mhd_rhs_q<BX, FIELD>(c, zo, P, roc, cur, Q);
-            else
-                acb::mhd_rhs<T, BX, FIELD>(c, zo, P, roc, cur);
-
             T fo[3] = {0, 0, 0};
-            if constexpr (STEP == 3)
-                acb::forcing_at<T>(a.P, i, j, k, fo);
-
-            if constexpr (CT) {
-                // from the centre slot the producer filled by TMA
-                const float* cs = centre + (size_t)(oq % Cfg::NC) * (Cfg::centre_slot_bytes() / 4) +
-                                  ty * TX + tx;
-                constexpr int FS = Cfg::TX * Cfg::TY;
+            if constexpr (QZ) {
+                // previous state and lo parts of this vertex: plain loads issued
+                // first, or (CT) read from the centre slot after the right-hand
+                // sides, which keeps their registers free through the stencils
+                CentreVals2 cv;
+                if constexpr (!CT)
+                    load_centre2<STEP>(L, out, in_lo, out_lo, id, cv);
+                const acb::F2* c = reinterpret_cast<const acb::F2*>(ring) + (size_t)sc * PLANE + col;
+                float roc[ACB_NF], cur[ACB_NF];
+                acb::F2 cur2[ACB_NARR];
+                acb::mhd_rhs_q<BX, FIELD>(c, zo, P, roc, cur, cur2, Q);
+                if constexpr (STEP == 3)
+                    acb::forcing_at<T>(a.P, i, j, k, fo);
+                if constexpr (CT) {
+                    // from the centre slot the producer filled by TMA
+                    const acb::F2* cs = reinterpret_cast<const acb::F2*>(centre) +
+                                        (size_t)(oq % Cfg::NC) * (Cfg::centre_slot_bytes() / 8) +
+                                        ty * TX + tx;
+                    constexpr int FS = Cfg::TX * Cfg::TY;
 #pragma unroll
-                for (int f = 0; f < ACB_NF; ++f) {
-                    if constexpr (CS::PREV)
-                        cv.prev[f] = cs[CS::POS_PREV * Cfg::CENTRE + f * FS];
+                    for (int ar = 0; ar < ACB_NARR; ++ar) {
+                        if constexpr (CS::PREV)
+                            cv.prev[ar] = cs[CS::POS_PREV * Cfg::CENTRE + ar * FS];
 #if ACB_MIXED
-                    cv.cur_lo[f] = cs[CS::POS_CUR_LO * Cfg::CENTRE + f * FS];
-                    if constexpr (CS::PREV)
-                        cv.prev_lo[f] = cs[CS::POS_PREV_LO * Cfg::CENTRE + f * FS];
-                    else
-                        cv.prev_lo[f] = 0.f;
+                        cv.cur_lo[ar] = cs[CS::POS_CUR_LO * Cfg::CENTRE + ar * FS];
+                        if constexpr (CS::PREV)
+                            cv.prev_lo[ar] = cs[CS::POS_PREV_LO * Cfg::CENTRE + ar * FS];
+                        else
+                            cv.prev_lo[ar] = acb::F2{0ull};
 #endif
+                    }
                 }
-            }
-
-#if ACB_MIXED
-            // The compensated update, two fields per instruction in the field
-            // pairs of the stencils (packed lanes; per lane the operations and
-            // rounding of pair_add):
-            //   d = rkB * roc (+ rkA * ((cur - prev) + (cur_lo - prev_lo)))
-            //   (hi, lo) = (cur, cur_lo) + d  [+ forcing of ux, uy, uz]
-            {
-                constexpr int FA[4] = {0, 1, 4, 3}, FB[4] = {7, 2, 5, 6};
+                // The update, two fields per instruction (one pair array):
+                //   FP32:  out = cur + rkA (cur - prev) + rkB roc  [+ forcing]
+                //   mixed: d = rkB roc (+ rkA ((cur - prev) + (cur_lo - prev_lo)))
+                //          (hi, lo) = (cur, cur_lo) + d, a two-sum  [+ forcing]
+                // Forcing acts on ux, uy, uz, lane 0 of arrays 1-3; the lane of
+                // ax, ay, az adds 0 (for the mixed pair, adding 0 to a pair that
+                // pair_add returned leaves it as it is).
                 const acb::F2 rkA2 = acb::pk2(rkA, rkA), rkB2 = acb::pk2(rkB, rkB);
+                acb::F2* o2 = reinterpret_cast<acb::F2*>(out);
+#if ACB_MIXED
+                acb::F2* ol2 = reinterpret_cast<acb::F2*>(out_lo);
+#endif
 #pragma unroll
-                for (int pr = 0; pr < 4; ++pr) {
-                    const int fa = FA[pr], fb = FB[pr];
-                    const acb::F2 c2 = acb::pk2(cur[fa], cur[fb]);
-                    const acb::F2 l2 = acb::pk2(cv.cur_lo[fa], cv.cur_lo[fb]);
-                    acb::F2 d2       = acb::mul2(rkB2, acb::pk2(roc[fa], roc[fb]));
+                for (int ar = 0; ar < ACB_NARR; ++ar) {
+                    const int fa = acb_field(ar, 0), fb = acb_field(ar, 1);
+                    const long long e = ar * L.fstride + id;
+                    const acb::F2 roc2 = acb::pk2(roc[fa], roc[fb]);
+#if ACB_MIXED
+                    const acb::F2 l2 = cv.cur_lo[ar];
+                    acb::F2 d2       = acb::mul2(rkB2, roc2);
                     if (STEP > 0) {
-                        const acb::F2 x =
-                            acb::add2(acb::sub2(c2, acb::pk2(cv.prev[fa], cv.prev[fb])),
-                                      acb::sub2(l2, acb::pk2(cv.prev_lo[fa], cv.prev_lo[fb])));
+                        const acb::F2 x = acb::add2(acb::sub2(cur2[ar], cv.prev[ar]),
+                                                    acb::sub2(l2, cv.prev_lo[ar]));
                         d2 = acb::fma2(rkA2, x, d2);
                     }
-                    acb::F2 h2, o2;
-                    acb::pair_add2(c2, l2, d2, h2, o2);
-                    if (STEP == 3 && (pr == 1 || pr == 3)) {
-                        // ux, uy; uz with az, whose lane adds 0 (a pair that
-                        // pair_add returned is left as it is by adding 0)
-                        const acb::F2 f2 =
-                            pr == 1 ? acb::pk2(fo[0], fo[1]) : acb::pk2(fo[2], 0.f);
-                        acb::pair_add2(h2, o2, f2, h2, o2);
-                    }
-                    float ha, hb, la, lb;
-                    acb::upk2(h2, ha, hb);
-                    acb::upk2(o2, la, lb);
-                    out[fa * L.fstride + id]    = ha;
-                    out[fb * L.fstride + id]    = hb;
-                    out_lo[fa * L.fstride + id] = la;
-                    out_lo[fb * L.fstride + id] = lb;
+                    acb::F2 h2, w2;
+                    acb::pair_add2(cur2[ar], l2, d2, h2, w2);
+                    if (STEP == 3 && ar >= 1)
+                        acb::pair_add2(h2, w2, acb::pk2(fo[ar - 1], 0.f), h2, w2);
+                    o2[e]  = h2;
+                    ol2[e] = w2;
+#else
+                    acb::F2 r;
+                    if (STEP == 0)
+                        r = acb::fma2(rkB2, roc2, cur2[ar]);
+                    else
+                        r = acb::fma2(rkB2, roc2,
+                                      acb::fma2(rkA2, acb::sub2(cur2[ar], cv.prev[ar]), cur2[ar]));
+                    if (STEP == 3 && ar >= 1)
+                        r = acb::add2(r, acb::pk2(fo[ar - 1], 0.f));
+                    o2[e] = r;
+#endif
+                }
+                (void)cur;
+            }
+            else {
+                // double precision: previous state loaded a plane ahead
+                CentreVals cv = cv_next;
+                if (p + 1 < tg.nout)
+                    load_centre<STEP>(L, out, id + L.plane, cv_next);
+                const state_t* c = reinterpret_cast<const state_t*>(ring) + (size_t)sc * PLANE + col;
+                T roc[ACB_NF], cur[ACB_NF];
+                acb::mhd_rhs<T, BX, FIELD>(c, zo, P, roc, cur);
+                if constexpr (STEP == 3)
+                    acb::forcing_at<T>(a.P, i, j, k, fo);
+#pragma unroll
+                for (int f = 0; f < ACB_NF; ++f) {
+                    T r;
+                    if (STEP == 0)
+                        r = cur[f] + rkB * roc[f];
+                    else
+                        r = cur[f] + rkA * (cur[f] - cv.prev[f]) + rkB * roc[f];
+                    if (STEP == 3 && f >= 1 && f <= 3)
+                        r += fo[f - 1];
+                    out[fidx(L, f, id)] = r;
                 }
             }
-#else
-#pragma unroll
-            for (int f = 0; f < ACB_NF; ++f) {
-                T r;
-                if (STEP == 0)
-                    r = cur[f] + rkB * roc[f];
-                else
-                    r = cur[f] + rkA * (cur[f] - cv.prev[f]) + rkB * roc[f];
-                if (STEP == 3 && f >= 1 && f <= 3)
-                    r += fo[f - 1];
-                out[f * L.fstride + id] = r;
-            }
-#endif
         }
         __syncwarp();
         // with the queues the centre plane is done with; without them the
@@ -1116,10 +1112,10 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     using T = AcReal;
     constexpr int TX = Cfg::TX, NP = Cfg::NP, BX = Cfg::BX;
     constexpr int FIELD = Cfg::FIELD, PLANE = Cfg::PLANE, CWARPS = Cfg::CWARPS;
-    constexpr uint32_t PLANE_BYTES = PLANE * sizeof(state_t);
+    constexpr uint32_t PLANE_BYTES = PLANE * ACB_ELEM;
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    state_t* ring = reinterpret_cast<state_t*>(smem_raw);
+    unsigned char* ring = smem_raw; // NP slots of PLANE_BYTES
     __shared__ __align__(8) uint64_t full[NP];
     __shared__ __align__(8) uint64_t empty[NP];
     // centre ring (CT): one slot per output plane, filled by the producer
@@ -1129,7 +1125,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     constexpr int NCS    = CT ? Cfg::NC : 1;
     __shared__ __align__(8) uint64_t full_c[NCS];
     __shared__ __align__(8) uint64_t empty_c[NCS];
-    float* centre = reinterpret_cast<float*>(smem_raw + Cfg::ring_bytes());
+    unsigned char* centre = smem_raw + Cfg::ring_bytes(); // NC slots of centre_slot_bytes
     __shared__ volatile int abort_flag;
     __shared__ SolveParams<T> sP[CWARPS]; // ensemble: each consumer warp's copy of its member's parameters
 
@@ -1200,7 +1196,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
                         break;
                     }
                     mbar_arrive_expect_tx(&full[s], PLANE_BYTES);
-                    tma_load_4d(ring + (size_t)s * PLANE, map, xt, yt, tg.k0 - NGHOST + l, 0,
+                    tma_load_4d(ring + (size_t)s * PLANE_BYTES, map, xt, yt, tg.k0 - NGHOST + l, 0,
                                 &full[s]);
                     ++q;
                     if constexpr (CT) {
@@ -1212,20 +1208,20 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
                                 ok = false;
                                 break;
                             }
-                            constexpr uint32_t CB = Cfg::CENTRE * sizeof(float);
-                            float* dst   = centre + (size_t)sc * (Cfg::centre_slot_bytes() / 4);
+                            constexpr uint32_t CB = Cfg::CENTRE * ACB_ELEM;
+                            unsigned char* dst = centre + (size_t)sc * Cfg::centre_slot_bytes();
                             const int xc = g->L.offx + tg.i0; // interior tile start: 32-byte aligned
                             const int zc = tg.k0 + (l - 2 * NGHOST);
                             mbar_arrive_expect_tx(&full_c[sc], CS::N * CB);
                             if (CS::PREV)
-                                tma_load_4d(dst + CS::POS_PREV * Cfg::CENTRE, &cm.m[0], xc, tg.j0,
-                                            zc, 0, &full_c[sc]);
+                                tma_load_4d(dst + CS::POS_PREV * CB, &cm.m[0], xc, tg.j0, zc, 0,
+                                            &full_c[sc]);
                             if (CS::LO)
-                                tma_load_4d(dst + CS::POS_CUR_LO * Cfg::CENTRE, &cm.m[1], xc,
-                                            tg.j0, zc, 0, &full_c[sc]);
+                                tma_load_4d(dst + CS::POS_CUR_LO * CB, &cm.m[1], xc, tg.j0, zc, 0,
+                                            &full_c[sc]);
                             if (CS::LO && CS::PREV)
-                                tma_load_4d(dst + CS::POS_PREV_LO * Cfg::CENTRE, &cm.m[2], xc,
-                                            tg.j0, zc, 0, &full_c[sc]);
+                                tma_load_4d(dst + CS::POS_PREV_LO * CB, &cm.m[2], xc, tg.j0, zc,
+                                            0, &full_c[sc]);
                             ++oq;
                         }
                     }
