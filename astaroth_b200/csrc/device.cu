@@ -289,8 +289,9 @@ acb_host::make_params(const AcMeshInfo& uniforms, const Layout& L, int step, int
             for (int k = 0; k < 4; ++k)
                 P.c2p[a][k] = dup(P.c2[a][k]);
         }
-        for (int k = 0; k < 3; ++k)
-            P.cxp[k] = dup(P.cx[0][k]);
+        for (int r = 0; r < 3; ++r)
+            for (int k = 0; k < 3; ++k)
+                P.cxp[r][k] = dup(P.cx[r][k]);
     }
 
     const double gamma = rp[AC_gamma], cp = rp[AC_cp_sound], mu0 = rp[AC_mu0];

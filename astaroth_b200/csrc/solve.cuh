@@ -45,9 +45,9 @@ struct SolveParams {
     T c1[3][3];   // first derivative: axis, k-1; pre-scaled by 1/ds
     T c2[3][4];   // second derivative: axis, {centre, k=1..3}; pre-scaled by 1/ds^2
     T cx[3][3];   // diagonal cross derivative: pair {xy, xz, yz}, k-1; pre-scaled
-    // single precision: c1, c2 and the xy row of cx as (c, c) pairs of FP32
-    // lanes, the coefficient operands of packed sums over two fields
-    unsigned long long c1p[3][3], c2p[3][4], cxp[3];
+    // single precision: c1, c2 and cx as (c, c) pairs of FP32 lanes, the
+    // coefficient operands of packed sums over the two fields of a pair
+    unsigned long long c1p[3][3], c2p[3][4], cxp[3][3];
     T nu, eta, inv_mu0, eta_mu0, zeta;
     T cs2_sound, inv_cp, gamma, gm1, gamma_inv_cp, lnrho0, lnT0, k_heat;
     T rkA, rkB; // out = cur + rkA * (cur - prev) + rkB * rate; rkA unused at s = 0
@@ -327,10 +327,11 @@ fma2(F2 a, F2 b, F2 c)
     return r;
 }
 
-// Register queue of one field along z (2.5D streaming): the values of the
-// thread's own column at the three planes below the current one and, for a
-// field with an xz (yz) cross derivative, the lower half of that derivative
-// as running sums. The diagonal cross derivative at plane z,
+// Register queue of one pair array along z (2.5D streaming): the (A, B)
+// values of the thread's own column at the three planes below the current one
+// and, where the pair has an xz (yz) cross derivative, the lower half of that
+// derivative as running sums, both fields in packed lanes. The diagonal cross
+// derivative at plane z,
 //   sum_k e_k (f(+k,+k) + f(-k,-k) - f(+k,-k) - f(-k,+k))
 //     = U(z) - L(z),  U(z) = sum_k e_k d_k(z+k),  L(z) = sum_k e_k d_k(z-k),
 // with d_k(w) = f(+k) - f(-k) the x (y) difference at plane w: the differences
@@ -340,88 +341,62 @@ fma2(F2 a, F2 b, F2 c)
 // and advancing a plane is three fused multiply-adds (no register moves):
 //   a1 <- e1 d1(z) + a2,  a2 <- e2 d2(z) + a3,  a3 <- e3 d3(z).
 // Only the upper half U is read from the ring.
-template <typename T>
-struct ZQueue {
-    T v1, v2, v3;    // f at z-1, z-2, z-3
-    T xa1, xa2, xa3; // xz lower half: L(z), partial L(z+1), partial L(z+2)
-    T ya1, ya2, ya3; // the same for yz
+struct PairQ {
+    F2 v1, v2, v3;    // (A, B) at z-1, z-2, z-3
+    F2 xa1, xa2, xa3; // xz lower half: L(z), partial L(z+1), partial L(z+2)
+    F2 ya1, ya2, ya3; // the same for yz
 };
 
-__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
-
 // Advances the lower-half sums of one z diagonal past the plane whose
-// differences are d1, d2, d3 (e: the diagonal's coefficients). The rounding
-// sequence is fixed (explicit fma / mul), so prime_pair below reproduces the
-// sums a streaming task would have built, bit for bit.
+// differences are d1, d2, d3 (e: the diagonal's (c, c) coefficient pairs).
+// The rounding sequence is fixed, so prime_pair below reproduces the sums a
+// streaming task would have built, bit for bit.
 __device__ __forceinline__ void
-zacc_push(float& a1, float& a2, float& a3, const float* e, float d1, float d2, float d3)
+zacc_push(F2& a1, F2& a2, F2& a3, const unsigned long long* e, F2 d1, F2 d2, F2 d3)
 {
-    a1 = fma_rn(e[0], d1, a2);
-    a2 = fma_rn(e[1], d2, a3);
-    a3 = mul_rn(e[2], d3);
+    a1 = fma2(F2{e[0]}, d1, a2);
+    a2 = fma2(F2{e[1]}, d2, a3);
+    a3 = mul2(F2{e[2]}, d3);
 }
 
-// Upper half U of one z diagonal (u1..u3: d_k at plane z+k), in the order
-// every caller uses.
-__device__ __forceinline__ float
-zacc_upper(const float* e, float u1, float u2, float u3)
+// Upper half U of one z diagonal (u1..u3: d_k at plane z+k).
+__device__ __forceinline__ F2
+zacc_upper(const unsigned long long* e, F2 u1, F2 u2, F2 u3)
 {
-    return fma_rn(e[2], u3, fma_rn(e[1], u2, mul_rn(e[0], u1)));
+    return fma2(F2{e[2]}, u3, fma2(F2{e[1]}, u2, mul2(F2{e[0]}, u1)));
 }
 
-// Lower-half sums of the z diagonals of both fields of a pair at the first
-// plane of a task from the three planes below it (zo[0..2]); step: 1 for xz,
-// the row pitch for yz. The differences are formed in packed lanes, as the
-// streaming plane forms them.
+// Lower-half sums of a z diagonal at the first plane of a task from the three
+// planes below it (zo[0..2]); step: 1 for xz, the row pitch for yz.
 __device__ __forceinline__ void
-zacc_prime2(const F2* __restrict__ c, const int* zo, int step, const float* e, float (&A)[3],
-            float (&B)[3])
+zacc_prime(const F2* __restrict__ c, const int* zo, int step, const unsigned long long* e, F2& a1,
+           F2& a2, F2& a3)
 {
-    float dA[3][4], dB[3][4]; // [plane z-3 + p][k]
-#pragma unroll
-    for (int p = 0; p < 3; ++p)
-#pragma unroll
-        for (int k = 1; k <= 3; ++k)
-            upk2(sub2(c[zo[p] + k * step], c[zo[p] - k * step]), dA[p][k], dB[p][k]);
-    auto prime = [&](const float (&d)[3][4], float (&a)[3]) {
-        // plane z-3: only its third difference reaches L(z)
-        const float t3 = mul_rn(e[2], d[0][3]);
-        // plane z-2
-        const float b2 = fma_rn(e[1], d[1][2], t3);
-        const float b3 = mul_rn(e[2], d[1][3]);
-        // plane z-1
-        a[0] = fma_rn(e[0], d[2][1], b2);
-        a[1] = fma_rn(e[1], d[2][2], b3);
-        a[2] = mul_rn(e[2], d[2][3]);
-    };
-    prime(dA, A);
-    prime(dB, B);
+    auto d = [&](int plane, int k) { return sub2(c[zo[plane] + k * step], c[zo[plane] - k * step]); };
+    // plane z-3: only its third difference reaches L(z)
+    const F2 t3 = mul2(F2{e[2]}, d(0, 3));
+    // plane z-2
+    const F2 b2 = fma2(F2{e[1]}, d(1, 2), t3);
+    const F2 b3 = mul2(F2{e[2]}, d(1, 3));
+    // plane z-1
+    a1 = fma2(F2{e[0]}, d(2, 1), b2);
+    a2 = fma2(F2{e[1]}, d(2, 2), b3);
+    a3 = mul2(F2{e[2]}, d(2, 3));
 }
 
-// Fills the queues of the fields of one pair array c from the ring at the
-// first plane of a task (zo[0..2]: the three planes below it). Both fields of
-// a pair have the same z diagonals (XZ, YZ).
+// Fills the queue of one pair array c from the ring at the first plane of a
+// task (zo[0..2]: the three planes below it).
 template <int BX, bool XZ, bool YZ>
 __device__ __forceinline__ void
-prime_pair(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P, ZQueue<float>& QA,
-           ZQueue<float>& QB)
+prime_pair(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P, PairQ& Q)
 {
-    upk2(c[zo[2]], QA.v1, QB.v1);
-    upk2(c[zo[1]], QA.v2, QB.v2);
-    upk2(c[zo[0]], QA.v3, QB.v3);
-    if (XZ) {
-        float A[3], B[3];
-        zacc_prime2(c, zo, 1, P.cx[1], A, B);
-        QA.xa1 = A[0], QA.xa2 = A[1], QA.xa3 = A[2];
-        QB.xa1 = B[0], QB.xa2 = B[1], QB.xa3 = B[2];
-    }
-    if (YZ) {
-        float A[3], B[3];
-        zacc_prime2(c, zo, BX, P.cx[2], A, B);
-        QA.ya1 = A[0], QA.ya2 = A[1], QA.ya3 = A[2];
-        QB.ya1 = B[0], QB.ya2 = B[1], QB.ya3 = B[2];
-    }
+    Q.v1 = c[zo[2]];
+    Q.v2 = c[zo[1]];
+    Q.v3 = c[zo[0]];
+    if (XZ)
+        zacc_prime(c, zo, 1, P.cxp[1], Q.xa1, Q.xa2, Q.xa3);
+    if (YZ)
+        zacc_prime(c, zo, BX, P.cxp[2], Q.ya1, Q.ya2, Q.ya3);
 }
 
 template <bool GX_, bool GY_, bool GZ_, bool XY_, bool XZ_, bool YZ_>
@@ -430,39 +405,36 @@ struct DFlags {
 };
 
 // The z-diagonal cross derivative of kind XK (xz, else yz) of both fields of
-// a pair: the upper-half differences in packed lanes (one 8-byte load per
-// point), the coefficient sums and the queued lower halves per field.
+// a pair, in packed lanes: upper half from the ring, lower half queued.
 template <bool XK, int BX>
 __device__ __forceinline__ void
-zcross_pair(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P,
-            const ZQueue<float>& QA, const ZQueue<float>& QB, float& sA, float& sB)
+zcross_pair(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P, const PairQ& Q,
+            float& sA, float& sB)
 {
     constexpr int step = XK ? 1 : BX;
-    const float* e     = P.cx[XK ? 1 : 2];
-    float a[3], b[3];
+    F2 u[3];
 #pragma unroll
     for (int k = 1; k <= 3; ++k) {
         const int z = zo[3 + k];
-        upk2(sub2(c[z + k * step], c[z - k * step]), a[k - 1], b[k - 1]);
+        u[k - 1]    = sub2(c[z + k * step], c[z - k * step]);
     }
-    sA = zacc_upper(e, a[0], a[1], a[2]) - (XK ? QA.xa1 : QA.ya1);
-    sB = zacc_upper(e, b[0], b[1], b[2]) - (XK ? QB.xa1 : QB.ya1);
+    const F2 s = sub2(zacc_upper(P.cxp[XK ? 1 : 2], u[0], u[1], u[2]), XK ? Q.xa1 : Q.ya1);
+    upk2(s, sA, sB);
 }
 
-// Advances a queue by one plane (after every use of it): f0 and the x / y
-// differences dx, dy of the plane just done.
+// Advances a pair's queue by one plane (after every use of it): F0 and the
+// x / y differences DX, DY of the plane just done.
 template <bool XZ, bool YZ>
 __device__ __forceinline__ void
-push_queue(ZQueue<float>& Q, const SolveParams<float>& P, float f0, const float* dx,
-           const float* dy)
+push_queue(PairQ& Q, const SolveParams<float>& P, F2 F0, const F2* DX, const F2* DY)
 {
     if (XZ)
-        zacc_push(Q.xa1, Q.xa2, Q.xa3, P.cx[1], dx[0], dx[1], dx[2]);
+        zacc_push(Q.xa1, Q.xa2, Q.xa3, P.cxp[1], DX[0], DX[1], DX[2]);
     if (YZ)
-        zacc_push(Q.ya1, Q.ya2, Q.ya3, P.cx[2], dy[0], dy[1], dy[2]);
+        zacc_push(Q.ya1, Q.ya2, Q.ya3, P.cxp[2], DY[0], DY[1], DY[2]);
     Q.v3 = Q.v2;
     Q.v2 = Q.v1;
-    Q.v1 = f0;
+    Q.v1 = F0;
 }
 
 // The derivatives of the two fields of one pair array c at once: every pencil
@@ -472,8 +444,7 @@ push_queue(ZQueue<float>& Q, const SolveParams<float>& P, float f0, const float*
 template <int BX, class FA, class FB>
 __device__ __forceinline__ void
 pair_derivs_q(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P,
-              ZQueue<float>& QA, ZQueue<float>& QB, FieldDerivs<float>& rA,
-              FieldDerivs<float>& rB, F2& F0)
+              PairQ& Q, FieldDerivs<float>& rA, FieldDerivs<float>& rB, F2& F0)
 {
     static_assert(FA::XY == FB::XY && FA::XZ == FB::XZ && FA::YZ == FB::YZ,
                   "the fields of a pair have the same cross derivatives");
@@ -498,56 +469,35 @@ pair_derivs_q(const F2* __restrict__ c, const int* zo, const SolveParams<float>&
         dsum(c[k], c[-k], DX[k - 1], SX[k - 1]);
         dsum(c[k * BX], c[-k * BX], DY[k - 1], SY[k - 1]);
     }
-    dsum(c[zo[4]], pk2(QA.v1, QB.v1), DZ[0], SZ[0]);
-    dsum(c[zo[5]], pk2(QA.v2, QB.v2), DZ[1], SZ[1]);
-    dsum(c[zo[6]], pk2(QA.v3, QB.v3), DZ[2], SZ[2]);
-    // Coefficient sums sum_k c_k d_k of both fields. The FP32 build forms them
-    // in packed lanes ((c, c) coefficient pairs; 2-3 % faster per step at
-    // 512^3); the mixed build, whose update holds more registers, runs 2 %
-    // faster with them in scalar form (the same operations per lane).
-    constexpr bool PACKED_SUMS = !ACB_MIXED;
-    auto sum3 = [&](const unsigned long long* cp, const float* cs, const F2* d, float& oa,
-                    float& ob) {
-        if constexpr (PACKED_SUMS) {
-            F2 r = mul2(F2{cp[0]}, d[0]);
-            r    = fma2(F2{cp[1]}, d[1], r);
-            upk2(fma2(F2{cp[2]}, d[2], r), oa, ob);
-        }
-        else {
-            float a[3], b[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-                upk2(d[k], a[k], b[k]);
-            oa = cs[0] * a[0] + cs[1] * a[1] + cs[2] * a[2];
-            ob = cs[0] * b[0] + cs[1] * b[1] + cs[2] * b[2];
-        }
+    dsum(c[zo[4]], Q.v1, DZ[0], SZ[0]);
+    dsum(c[zo[5]], Q.v2, DZ[1], SZ[1]);
+    dsum(c[zo[6]], Q.v3, DZ[2], SZ[2]);
+    // Coefficient sums sum_k c_k d_k of both fields at once, with (c, c)
+    // coefficient pairs from the kernel parameters.
+    auto sum3 = [&](const unsigned long long* cp, const F2* d, float& oa, float& ob) {
+        F2 r = mul2(F2{cp[0]}, d[0]);
+        r    = fma2(F2{cp[1]}, d[1], r);
+        upk2(fma2(F2{cp[2]}, d[2], r), oa, ob);
     };
     float gA, gB;
     if (FA::GX || FB::GX) {
-        sum3(P.c1p[0], P.c1[0], DX, gA, gB);
+        sum3(P.c1p[0], DX, gA, gB);
         if (FA::GX) rA.gx = gA;
         if (FB::GX) rB.gx = gB;
     }
     if (FA::GY || FB::GY) {
-        sum3(P.c1p[1], P.c1[1], DY, gA, gB);
+        sum3(P.c1p[1], DY, gA, gB);
         if (FA::GY) rA.gy = gA;
         if (FB::GY) rB.gy = gB;
     }
     if (FA::GZ || FB::GZ) {
-        sum3(P.c1p[2], P.c1[2], DZ, gA, gB);
+        sum3(P.c1p[2], DZ, gA, gB);
         if (FA::GZ) rA.gz = gA;
         if (FB::GZ) rB.gz = gB;
     }
-    sum3(P.c2p[0] + 1, P.c2[0] + 1, SX, rA.xx, rB.xx);
-    sum3(P.c2p[1] + 1, P.c2[1] + 1, SY, rA.yy, rB.yy);
-    sum3(P.c2p[2] + 1, P.c2[2] + 1, SZ, rA.zz, rB.zz);
-    // the x and y differences of this plane, for the z-diagonal queues
-    float dxA[3], dxB[3], dyA[3], dyB[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        upk2(DX[k], dxA[k], dxB[k]);
-        upk2(DY[k], dyA[k], dyB[k]);
-    }
+    sum3(P.c2p[0] + 1, SX, rA.xx, rB.xx);
+    sum3(P.c2p[1] + 1, SY, rA.yy, rB.yy);
+    sum3(P.c2p[2] + 1, SZ, rA.zz, rB.zz);
 
     // xy diagonals (the whole stencil from the centre plane)
     if (FA::XY) {
@@ -557,17 +507,16 @@ pair_derivs_q(const F2* __restrict__ c, const int* zo, const SolveParams<float>&
             const int pp = k + k * BX, mm = -k - k * BX, pm = k - k * BX, mp = -k + k * BX;
             E[k - 1] = sub2(add2(c[pp], c[mm]), add2(c[pm], c[mp]));
         }
-        sum3(P.cxp, P.cx[0], E, rA.xy, rB.xy);
+        sum3(P.cxp[0], E, rA.xy, rB.xy);
     }
 
     // z diagonals (both fields have the same kinds)
     if (FA::XZ)
-        zcross_pair<true, BX>(c, zo, P, QA, QB, rA.xz, rB.xz);
+        zcross_pair<true, BX>(c, zo, P, Q, rA.xz, rB.xz);
     if (FA::YZ)
-        zcross_pair<false, BX>(c, zo, P, QA, QB, rA.yz, rB.yz);
+        zcross_pair<false, BX>(c, zo, P, Q, rA.yz, rB.yz);
 
-    push_queue<FA::XZ, FA::YZ>(QA, P, a0, dxA, dyA);
-    push_queue<FB::XZ, FB::YZ>(QB, P, b0, dxB, dyB);
+    push_queue<FA::XZ, FA::YZ>(Q, P, F0, DX, DY);
 }
 
 // Derivative flags of the eight fields: what the right-hand sides use.
@@ -612,29 +561,29 @@ mhd_rhs(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, T
 template <int BX, int FIELD>
 __device__ __forceinline__ void
 mhd_rhs_q(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P,
-          float roc[ACB_NF], float cur[ACB_NF], F2 cur2[ACB_NARR], ZQueue<float> (&Q)[ACB_NF])
+          float roc[ACB_NF], float cur[ACB_NF], F2 cur2[ACB_NARR], PairQ (&Q)[ACB_NARR])
 {
     FieldDerivs<float> lr, ux, uy, uz, ax, ay, az, ss;
-    pair_derivs_q<BX, DFlags<ACB_D_LNRHO>, DFlags<ACB_D_SS>>(c + 0 * FIELD, zo, P, Q[0], Q[7], lr,
-                                                             ss, cur2[0]);
-    pair_derivs_q<BX, DFlags<ACB_D_UUX>, DFlags<ACB_D_AX>>(c + 1 * FIELD, zo, P, Q[1], Q[4], ux,
-                                                           ax, cur2[1]);
-    pair_derivs_q<BX, DFlags<ACB_D_UUY>, DFlags<ACB_D_AY>>(c + 2 * FIELD, zo, P, Q[2], Q[5], uy,
-                                                           ay, cur2[2]);
-    pair_derivs_q<BX, DFlags<ACB_D_UUZ>, DFlags<ACB_D_AZ>>(c + 3 * FIELD, zo, P, Q[3], Q[6], uz,
-                                                           az, cur2[3]);
+    pair_derivs_q<BX, DFlags<ACB_D_LNRHO>, DFlags<ACB_D_SS>>(c + 0 * FIELD, zo, P, Q[0], lr, ss,
+                                                             cur2[0]);
+    pair_derivs_q<BX, DFlags<ACB_D_UUX>, DFlags<ACB_D_AX>>(c + 1 * FIELD, zo, P, Q[1], ux, ax,
+                                                           cur2[1]);
+    pair_derivs_q<BX, DFlags<ACB_D_UUY>, DFlags<ACB_D_AY>>(c + 2 * FIELD, zo, P, Q[2], uy, ay,
+                                                           cur2[2]);
+    pair_derivs_q<BX, DFlags<ACB_D_UUZ>, DFlags<ACB_D_AZ>>(c + 3 * FIELD, zo, P, Q[3], uz, az,
+                                                           cur2[3]);
     rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
 }
 
 template <int BX, int FIELD>
 __device__ __forceinline__ void
 prime_queues(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P,
-             ZQueue<float> (&Q)[ACB_NF])
+             PairQ (&Q)[ACB_NARR])
 {
-    prime_pair<BX, false, false>(c + 0 * FIELD, zo, P, Q[0], Q[7]);
-    prime_pair<BX, true, false>(c + 1 * FIELD, zo, P, Q[1], Q[4]);
-    prime_pair<BX, false, true>(c + 2 * FIELD, zo, P, Q[2], Q[5]);
-    prime_pair<BX, true, true>(c + 3 * FIELD, zo, P, Q[3], Q[6]);
+    prime_pair<BX, false, false>(c + 0 * FIELD, zo, P, Q[0]);
+    prime_pair<BX, true, false>(c + 1 * FIELD, zo, P, Q[1]);
+    prime_pair<BX, false, true>(c + 2 * FIELD, zo, P, Q[2]);
+    prime_pair<BX, true, true>(c + 3 * FIELD, zo, P, Q[3]);
 }
 
 // Right-hand sides from the derivative sets (stencil_kernel.ac:355-528,
@@ -916,7 +865,7 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
     // arrays; double precision has no registers to spare for them and reads
     // every operand from the ring
     constexpr bool QZ = ACB_PAIRED;
-    acb::ZQueue<float> Q[ACB_NF];
+    acb::PairQ Q[ACB_NARR];
     if constexpr (QZ) {
         if (ok && act) {
             const uint32_t sc = (q + NGHOST) % NP;
