@@ -5,8 +5,10 @@
 //
 // Differences of design from the reference, all invisible at the interface:
 //   - the eight fields of `in` (and of `out`) live in one allocation with a
-//     padded row pitch (common.cuh: Layout); load/store translate between the
-//     caller's flat mx*my*mz arrays and that layout with pitched copies;
+//     padded row pitch, in single precision as four arrays of interleaved
+//     field pairs (common.cuh: Layout, fidx); load/store translate between the
+//     caller's flat mx*my*mz arrays and that layout through a device staging
+//     buffer and a scatter / gather kernel;
 //   - the run-time parameters ("uniforms") are a per-Device host mirror of
 //     AcMeshInfo, turned into pre-scaled kernel arguments at each launch,
 //     instead of one __constant__ AcMeshInfo per GPU; loads keep the

@@ -97,11 +97,13 @@ SolveParams<AcReal> make_params(const AcMeshInfo& uniforms, const Layout& L, int
 // z segments per tile column so that tiles*segments fills the last wave best
 int choose_segments(long long ntiles, int nzr, long long slots, int min_planes);
 
-// Device staging buffer of loads: the caller's values are copied into it in
-// one contiguous transfer per chunk and a kernel scatters them into the padded
-// rows (a pitched host-to-device copy of rows a few KB long runs at about a
-// third of the contiguous rate). `done` is recorded after each use, and the
-// next use, on whatever stream, waits for it.
+// Device staging buffer of loads and stores: the caller's values pass through
+// it in one contiguous transfer per chunk, and a kernel scatters them into (or
+// gathers them from) the padded layout, where a field's values are ACB_LANES
+// apart (a pitched host-to-device copy of rows a few KB long ran at about a
+// third of the contiguous rate, and the pair layout interleaves two fields).
+// `done` is recorded after each use, and the next use, on whatever stream,
+// waits for it.
 struct StageBuf {
     state_t* buf;
     size_t elems;
@@ -111,9 +113,9 @@ struct StageBuf {
 AcResult stage_create(StageBuf* stage, size_t max_elems);
 void stage_destroy(StageBuf* stage);
 
-// copies a flat range of a field between host memory (reference order) and
-// the padded device layout; zeroes the lo parts of loaded values when given.
-// Loads go through the staging buffer when one is given.
+// copies a flat range of a field (field: its base, block + fidx(L, f, 0))
+// between host memory (reference order) and the padded device layout through
+// the staging buffer; zeroes the lo parts of loaded values when given.
 AcResult copy_field_range(cudaStream_t st, const Layout& L, state_t* field, size_t s,
                           AcReal* host, size_t count, bool h2d, float* lo_field,
                           StageBuf* stage);
