@@ -14,15 +14,16 @@ using SolveCfg0 = TileCfg<32, 4, 8, 1>;
 using SolveCfg1 = TileCfg<16, 8, 8, 1>;
 using SolveCfg2 = TileCfg<32, 2, 10, 2>;
 #elif ACB_MIXED
-// the first two stage the centre values of substeps 1 and 2 by TMA; the first
-// (the default) is the fastest on the 512^3 workload in the paired layout
-using SolveCfg0 = TileCfg<64, 4, 6, 1, 3>;
-using SolveCfg1 = TileCfg<32, 8, 7, 1, 3>;
-using SolveCfg2 = TileCfg<32, 8, 9, 1>;
+// all three stage the centre values of substeps 1 and 2 by TMA; the first (the
+// default, 12 consumer warps) is the fastest on the 512^3 workload
+using SolveCfg0 = TileCfg<32, 12, 6, 1, 2>;
+using SolveCfg1 = TileCfg<64, 4, 6, 1, 3>;
+using SolveCfg2 = TileCfg<32, 8, 7, 1, 3>;
 #else
-using SolveCfg0 = TileCfg<32, 8, 9, 1>;
-using SolveCfg1 = TileCfg<64, 4, 8, 1>;
-using SolveCfg2 = TileCfg<32, 8, 7, 1>;
+// the first (the default, 12 consumer warps) is the fastest at 512^3
+using SolveCfg0 = TileCfg<64, 6, 7, 1>;
+using SolveCfg1 = TileCfg<32, 8, 9, 1>;
+using SolveCfg2 = TileCfg<64, 4, 8, 1>;
 #endif
 
 typedef void (*SolveKernelFn)(const CUtensorMap, const SolveArgs<AcReal>, const CentreMaps);

@@ -22,15 +22,19 @@
 //     into a ring of NP plane slots in shared memory (mbarrier `full` with
 //     transaction bytes); consumer warps release a slot through an `empty`
 //     mbarrier when done, so no block-wide barrier sits in the plane loop;
+//   - single precision: the layout interleaves the fields in pairs with the
+//     same stencils, (lnrho, ss), (ux, ax), (uy, ay), (uz, az), so a stencil
+//     point of a pair is one 8-byte shared load and its arithmetic runs in
+//     packed f32x2 lanes;
 //   - one consumer thread per (x, y) column; in single precision each thread
 //     keeps a register queue along z (its column's values of the three planes
-//     below, and the x / y differences the xz / yz diagonals need from them),
+//     below, and running sums of the lower halves of the xz / yz diagonals),
 //     so the ring is read for the centre plane and the three above it only
-//     (224 instead of 296 shared-memory reads per vertex) and a plane's slot is
-//     released as soon as its own outputs are done; double precision reads all
-//     seven planes from the ring; the centre-only values (previous state, lo
-//     parts) are loaded from global memory at the top of each plane (a plane
-//     ahead in double precision);
+//     (112 8-byte shared loads per vertex instead of 296 values) and a plane's
+//     slot is released as soon as its own outputs are done; double precision
+//     reads all seven planes from the ring; the centre-only values (previous
+//     state, lo parts) arrive by TMA in a ring of output-plane slots (mixed
+//     substeps 1 and 2) or by plain loads (a plane ahead in double precision);
 //   - derivative coefficients arrive pre-scaled by 1/ds (and 1/ds^2) so each
 //     pencil costs 6-7 FP ops; only the 21 first, 24 second and 12 cross
 //     derivatives the right-hand sides use are formed;
@@ -127,14 +131,16 @@ struct TileCfg {
     static constexpr int BX = TX_ + 8, BY = TY_ + 6;
     static constexpr int CONSUMERS = TX_ * TY_;        // one thread per (x, y) column
     static constexpr int CWARPS    = CONSUMERS / 32;   // consumer warps
-    // Single precision with 8 consumer warps: the producer is a whole
+    // Single precision with 8 or 12 consumer warps: the producer is a whole
     // warpgroup (4 warps, one of them working) that hands its registers to the
-    // consumers (setmaxnreg), so each consumer thread gets 232 registers for
-    // its z queues. An SM sub-partition's 16K registers hold 2 consumer warps
-    // and 1 producer warp: 2 * 232 + 40 = 504 <= 512 registers a lane.
-    static constexpr bool WGSPEC   = sizeof(state_t) == 4 && CWARPS == 8;
-    static constexpr int THREADS   = CONSUMERS + (WGSPEC ? 128 : 32); // plus the producer
-    static constexpr int REG_CONSUMER = 232, REG_PRODUCER = 40;
+    // consumers (setmaxnreg), so each consumer thread gets the registers its z
+    // queues need. An SM sub-partition's 16K registers hold 2 consumer warps
+    // and 1 producer warp (2 * 232 + 40 = 504 <= 512 registers a lane), or 3
+    // and 1 (3 * 160 + 32 = 512): more warps to hide latency, fewer registers.
+    static constexpr bool WGSPEC = sizeof(state_t) == 4 && (CWARPS == 8 || CWARPS == 12);
+    static constexpr int THREADS = CONSUMERS + (WGSPEC ? 128 : 32); // plus the producer
+    static constexpr int REG_CONSUMER = CWARPS == 12 ? 160 : 232;
+    static constexpr int REG_PRODUCER = CWARPS == 12 ? 32 : 40;
     // registers a thread the launch must hold for the reallocation to balance
     static constexpr int REG_LAUNCH =
         WGSPEC ? (REG_CONSUMER * CONSUMERS + REG_PRODUCER * 128 + THREADS - 1) / THREADS : 0;
@@ -146,6 +152,13 @@ struct TileCfg {
         return (size_t)(ACB_MIXED ? 3 : 1) * CENTRE * ACB_ELEM;
     }
     static constexpr size_t smem_bytes() { return ring_bytes() + NC * centre_slot_bytes(); }
+    // A task starts once the first 2 NGHOST planes are in the ring (the queue
+    // priming and the first output plane's upper half), and without queues an
+    // output plane needs all 2 NGHOST + 1 of its planes at once: a shallower
+    // ring could never hold them.
+    static_assert(NP >= (sizeof(state_t) == 4 ? 2 * NGHOST : 2 * NGHOST + 1),
+                  "ring too shallow for the planes a task waits for");
+    static_assert(smem_bytes() <= 227 * 1024, "shared memory of one CTA exceeded");
 };
 
 namespace acb {
