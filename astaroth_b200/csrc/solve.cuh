@@ -471,11 +471,19 @@ pair_derivs_q(const F2* __restrict__ c, const int* zo, const SolveParams<float>&
     // smooth field u and v are exact in FP32 (Sterbenz), so f(+k) + f(-k) - 2 f0
     // keeps its digits instead of cancelling terms of size |c0 f0| (about
     // 2.7 f / ds^2); mathematically the same stencil (c0 = -2 (c1 + c2 + c3)).
+    // The FP32 build, whose error is that of its FP32 state, keeps the plain
+    // sums f(+k) + f(-k) and adds c0 f0 (two packed operations per point pair
+    // instead of three); the difference form is what brings the mixed build
+    // within 2.2e-7 of FP64.
     // First differences f(+k) - f(-k) directly, as prime_pair forms the queued
     // ones, so results do not depend on where a task's z segment starts.
+    constexpr bool DIFF_FORM = ACB_MIXED != 0;
     auto dsum = [&](F2 p, F2 m, F2& D, F2& S) {
         D = sub2(p, m);
-        S = add2(sub2(p, F0), sub2(m, F0));
+        if constexpr (DIFF_FORM)
+            S = add2(sub2(p, F0), sub2(m, F0));
+        else
+            S = add2(p, m);
     };
 #pragma unroll
     for (int k = 1; k <= 3; ++k) {
@@ -508,9 +516,23 @@ pair_derivs_q(const F2* __restrict__ c, const int* zo, const SolveParams<float>&
         if (FA::GZ) rA.gz = gA;
         if (FB::GZ) rB.gz = gB;
     }
-    sum3(P.c2p[0] + 1, SX, rA.xx, rB.xx);
-    sum3(P.c2p[1] + 1, SY, rA.yy, rB.yy);
-    sum3(P.c2p[2] + 1, SZ, rA.zz, rB.zz);
+    if constexpr (DIFF_FORM) {
+        sum3(P.c2p[0] + 1, SX, rA.xx, rB.xx);
+        sum3(P.c2p[1] + 1, SY, rA.yy, rB.yy);
+        sum3(P.c2p[2] + 1, SZ, rA.zz, rB.zz);
+    }
+    else {
+        // c0 f0 + sum_k c_k (f(+k) + f(-k))
+        auto sum4 = [&](const unsigned long long* cp, const F2* d, float& oa, float& ob) {
+            F2 r = mul2(F2{cp[0]}, F0);
+            r    = fma2(F2{cp[1]}, d[0], r);
+            r    = fma2(F2{cp[2]}, d[1], r);
+            upk2(fma2(F2{cp[3]}, d[2], r), oa, ob);
+        };
+        sum4(P.c2p[0], SX, rA.xx, rB.xx);
+        sum4(P.c2p[1], SY, rA.yy, rB.yy);
+        sum4(P.c2p[2], SZ, rA.zz, rB.zz);
+    }
 
     // xy diagonals (the whole stencil from the centre plane)
     if (FA::XY) {
