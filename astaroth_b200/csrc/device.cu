@@ -411,7 +411,7 @@ launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e)
     a.status     = d->status;
     a.P          = make_params(d->uniforms, d->L, step, d->forcing);
 
-    const SolveKernelFn kern = cfg.kern[step == 2 && d->forcing ? 3 : step];
+    const SolveKernelFn kern = (SolveKernelFn)cfg.kern[step == 2 && d->forcing ? 3 : step];
     int per_sm = 0;
     ACB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern,
                                                                  cfg.threads, cfg.smem));

@@ -15,6 +15,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -106,6 +107,10 @@ struct ensemble_s {
 
     bool desc_valid;
     std::vector<MemberDesc<AcReal>> h_desc[2];
+    std::vector<MemberParams<AcReal>> h_mp; // by task-list position (both parities)
+    // launch arguments of one group of members (about 20 KB, kept off the
+    // stack; the launch copies them)
+    std::unique_ptr<EnsSolveArgs<AcReal>> args;
     MemberDesc<AcReal>* d_desc[2];
     HaloMember* d_halo[2];
     long long halo_total; // work units of one batched ghost fill
@@ -122,6 +127,39 @@ struct ensemble_s {
 };
 
 namespace {
+
+// The parts of a member's kernel parameters that its stencils and right-hand
+// sides read (MemberParams), from its full parameter set.
+MemberParams<AcReal>
+member_params(const SolveParams<AcReal>& P)
+{
+    MemberParams<AcReal> m;
+    memset(&m, 0, sizeof(m));
+#if AC_DOUBLE_PRECISION == 1
+    memcpy(m.c1, P.c1, sizeof(m.c1));
+    memcpy(m.c2, P.c2, sizeof(m.c2));
+    memcpy(m.cx, P.cx, sizeof(m.cx));
+#else
+    memcpy(m.c1p, P.c1p, sizeof(m.c1p));
+    memcpy(m.c2p, P.c2p, sizeof(m.c2p));
+    memcpy(m.cxp, P.cxp, sizeof(m.cxp));
+#endif
+    m.nu           = P.nu;
+    m.eta          = P.eta;
+    m.inv_mu0      = P.inv_mu0;
+    m.eta_mu0      = P.eta_mu0;
+    m.zeta         = P.zeta;
+    m.cs2_sound    = P.cs2_sound;
+    m.inv_cp       = P.inv_cp;
+    m.gamma        = P.gamma;
+    m.gm1          = P.gm1;
+    m.gamma_inv_cp = P.gamma_inv_cp;
+    m.lnrho0       = P.lnrho0;
+    m.lnT0         = P.lnT0;
+    m.k_heat       = P.k_heat;
+    return m;
+}
+
 
 void
 drop_graphs(Ensemble e)
@@ -149,6 +187,7 @@ build_tables(Ensemble e)
     ACB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.kern[1], cfg.threads,
                                                                  cfg.smem));
     per_sm = std::max(per_sm, 1);
+    e->h_mp.assign(n, MemberParams<AcReal>());
     for (int p = 0; p < 2; ++p) {
         std::vector<MemberDesc<AcReal>>& D = e->h_desc[p];
         D.assign(n, MemberDesc<AcReal>());
@@ -194,7 +233,8 @@ build_tables(Ensemble e)
             d.out         = mb.blk[p ^ 1];
             d.in_lo       = mb.lo[p];
             d.out_lo      = mb.lo[p ^ 1];
-            d.P           = make_params(mb.uniforms, L, 0, 0);
+            if (p == 0)
+                e->h_mp[pos] = member_params(make_params(mb.uniforms, L, 0, 0));
             H[pos].L          = L;
             H[pos].block      = mb.blk[p];
             H[pos].lo         = nullptr; // lo parts of ghosts: never read in an ensemble
@@ -233,7 +273,12 @@ launch_solve_all(Ensemble e, cudaStream_t st, int step, AcReal dt)
 {
     int ncfg;
     const SolveConfig& cfg = ensemble_configs(&ncfg)[e->cfg];
-    SolveArgs<AcReal> a;
+    const int n            = (int)e->m.size();
+    // the launch arguments carry up to ACB_ENS_GROUP members' parameters, so
+    // a larger ensemble takes one launch per group of members (in task order)
+    if (!e->args)
+        e->args.reset(new EnsSolveArgs<AcReal>());
+    EnsSolveArgs<AcReal>& a = *e->args;
     memset(&a, 0, sizeof(a));
     // Williamson (1980) 2N coefficients, "previous state" form (as the Device path)
     const double alpha[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
@@ -241,16 +286,26 @@ launch_solve_all(Ensemble e, cudaStream_t st, int step, AcReal dt)
     a.P.rkB               = (AcReal)(beta[step] * (double)dt);
     a.P.rkA               = step > 0 ? (AcReal)(beta[step] * alpha[step] / beta[step - 1]) : 0;
     a.status              = e->status;
-    a.members             = e->d_desc[e->cur];
-    a.nmembers            = (int)e->m.size();
-    a.total_tasks         = e->total_tasks;
-    // the map parameter is not read in ensemble mode; any valid map fills it
     // ensemble kernels take their centre values by plain loads: no centre maps
     static const CentreMaps no_centre_maps = {};
-    cfg.kern[step]<<<e->grid, cfg.threads, cfg.smem, st>>>(e->h_desc[e->cur][0].tmap, a,
-                                                            no_centre_maps);
-    ACB_CUDA_CHECK(cudaGetLastError());
-    e->launches++;
+    const std::vector<MemberDesc<AcReal>>& D = e->h_desc[e->cur];
+    for (int g0 = 0; g0 < n; g0 += ACB_ENS_GROUP) {
+        const int gn            = std::min(ACB_ENS_GROUP, n - g0);
+        const long long t_begin = D[g0].task_begin;
+        const long long t_end   = g0 + gn < n ? D[g0 + gn].task_begin : e->total_tasks;
+        a.members               = e->d_desc[e->cur] + g0;
+        a.nmembers              = gn;
+        a.task_base             = t_begin;
+        a.total_tasks           = t_end - t_begin;
+        for (int i = 0; i < gn; ++i)
+            a.mp[i] = e->h_mp[g0 + i];
+        const int grid = (int)std::min<long long>(e->grid, a.total_tasks);
+        // the map parameter is not read in ensemble mode; any valid map fills it
+        ((EnsKernelFn)cfg.kern[step])<<<grid, cfg.threads, cfg.smem, st>>>(D[0].tmap, a,
+                                                                           no_centre_maps);
+        ACB_CUDA_CHECK(cudaGetLastError());
+        e->launches++;
+    }
     e->ghost_ok[e->cur ^ 1] = false; // the out blocks' ghosts are stale now
     return AC_SUCCESS;
 }

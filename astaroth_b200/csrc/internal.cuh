@@ -27,6 +27,7 @@ using SolveCfg2 = TileCfg<64, 4, 8, 1>;
 #endif
 
 typedef void (*SolveKernelFn)(const CUtensorMap, const SolveArgs<AcReal>, const CentreMaps);
+typedef void (*EnsKernelFn)(const CUtensorMap, const EnsSolveArgs<AcReal>, const CentreMaps);
 
 struct SolveConfig {
     const char* name;
@@ -34,7 +35,9 @@ struct SolveConfig {
     int launch_regs; // registers a thread the kernels must be launched with (0: any)
     int NC;          // centre ring slots (0: the centre values are plain loads)
     size_t smem;
-    SolveKernelFn kern[4]; // substeps 0, 1, 2, and 2 with helical forcing (single mesh only)
+    // substeps 0, 1, 2, and 2 with helical forcing (single mesh only): a
+    // SolveKernelFn, or an EnsKernelFn in the ensemble table
+    const void* kern[4];
 };
 
 // "tile32x8_ring9", "..._tmacentre" when the centre values are staged by TMA
@@ -62,13 +65,13 @@ make_solve_config()
     c.launch_regs = Cfg::REG_LAUNCH;
     c.NC          = ENS ? 0 : Cfg::NC;
     c.smem    = ENS ? Cfg::ring_bytes() : Cfg::smem_bytes(); // ensembles load centres directly
-    c.kern[0] = solve_kernel<Cfg, 0, ENS>;
-    c.kern[1] = solve_kernel<Cfg, 1, ENS>;
-    c.kern[2] = solve_kernel<Cfg, 2, ENS>;
+    c.kern[0] = (const void*)solve_kernel<Cfg, 0, ENS>;
+    c.kern[1] = (const void*)solve_kernel<Cfg, 1, ENS>;
+    c.kern[2] = (const void*)solve_kernel<Cfg, 2, ENS>;
     if constexpr (ENS)
         c.kern[3] = nullptr;
     else
-        c.kern[3] = solve_kernel<Cfg, 3, ENS>;
+        c.kern[3] = (const void*)solve_kernel<Cfg, 3, ENS>;
     return c;
 }
 

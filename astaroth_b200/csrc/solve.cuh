@@ -41,6 +41,8 @@
 //   - the mixed build keeps the state as an unevaluated float pair (hi, lo):
 //     stencils read hi, the update is a compensated two-sum.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 #include "tma.cuh"
 
@@ -73,8 +75,9 @@ struct SolveGeom {
 };
 
 // One member of an ensemble (many independent meshes advanced by one launch):
-// the TMA map of its `in` block, its geometry and task range, its buffers and
-// its parameters. Kept in global memory, one table per buffer parity.
+// the TMA map of its `in` block, its geometry and task range and its buffers.
+// Kept in global memory, one table per buffer parity; its parameters travel
+// with the launch (MemberParams below).
 template <typename T>
 struct __align__(128) MemberDesc {
     CUtensorMap tmap;
@@ -83,7 +86,6 @@ struct __align__(128) MemberDesc {
     state_t* out;
     float* in_lo;
     float* out_lo;
-    SolveParams<T> P; // rkA / rkB / forcing are taken from the launch, not from here
 };
 
 template <typename T>
@@ -98,6 +100,35 @@ struct SolveArgs {
     const MemberDesc<T>* members;
     int nmembers;
     long long total_tasks;
+};
+
+// Parameters of one ensemble member as the stencils and right-hand sides read
+// them, carried in the launch's parameter space (the constant bank, as a single
+// mesh's SolveParams are) instead of being read from memory at every use.
+template <typename T>
+struct MemberParams;
+template <>
+struct MemberParams<float> {
+    unsigned long long c1p[3][3], c2p[3][4], cxp[3][3]; // (c, c) coefficient pairs
+    float nu, eta, inv_mu0, eta_mu0, zeta;
+    float cs2_sound, inv_cp, gamma, gm1, gamma_inv_cp, lnrho0, lnT0, k_heat;
+};
+template <>
+struct MemberParams<double> {
+    double c1[3][3], c2[3][4], cx[3][3];
+    double nu, eta, inv_mu0, eta_mu0, zeta;
+    double cs2_sound, inv_cp, gamma, gm1, gamma_inv_cp, lnrho0, lnT0, k_heat;
+};
+
+// Members per ensemble launch (a launch's parameters stay within 32 KB; a
+// larger ensemble takes one launch per group of members).
+constexpr int ACB_ENS_GROUP = 64;
+
+template <typename T>
+struct EnsSolveArgs : SolveArgs<T> {
+    long long task_base;                 // first task of the group (tasks of all groups
+                                         // are numbered as one list, member-major)
+    MemberParams<T> mp[ACB_ENS_GROUP];   // by position in the group
 };
 
 // Centre-only arrays of a substep that the ring does not carry: the previous
@@ -217,9 +248,9 @@ struct FieldDerivs {
 
 // c: pointer to the field's centre element in the centre slot;
 // zo[0..6]: element offsets of the slots of planes z-3 .. z+3 from the centre slot.
-template <typename T, int BX, bool GX, bool GY, bool GZ, bool XY, bool XZ, bool YZ>
+template <typename T, int BX, bool GX, bool GY, bool GZ, bool XY, bool XZ, bool YZ, class PT>
 __device__ __forceinline__ FieldDerivs<T>
-field_derivs(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P)
+field_derivs(const state_t* __restrict__ c, const int* zo, const PT& P)
 {
     FieldDerivs<T> r;
     const T f0 = (T)c[0];
@@ -399,9 +430,9 @@ zacc_prime(const F2* __restrict__ c, const int* zo, int step, const unsigned lon
 
 // Fills the queue of one pair array c from the ring at the first plane of a
 // task (zo[0..2]: the three planes below it).
-template <int BX, bool XZ, bool YZ>
+template <int BX, bool XZ, bool YZ, class PT>
 __device__ __forceinline__ void
-prime_pair(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P, PairQ& Q)
+prime_pair(const F2* __restrict__ c, const int* zo, const PT& P, PairQ& Q)
 {
     Q.v1 = c[zo[2]];
     Q.v2 = c[zo[1]];
@@ -419,9 +450,9 @@ struct DFlags {
 
 // The z-diagonal cross derivative of kind XK (xz, else yz) of both fields of
 // a pair, in packed lanes: upper half from the ring, lower half queued.
-template <bool XK, int BX>
+template <bool XK, int BX, class PT>
 __device__ __forceinline__ void
-zcross_pair(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P, const PairQ& Q,
+zcross_pair(const F2* __restrict__ c, const int* zo, const PT& P, const PairQ& Q,
             float& sA, float& sB)
 {
     constexpr int step = XK ? 1 : BX;
@@ -437,9 +468,9 @@ zcross_pair(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P
 
 // Advances a pair's queue by one plane (after every use of it): F0 and the
 // x / y differences DX, DY of the plane just done.
-template <bool XZ, bool YZ>
+template <bool XZ, bool YZ, class PT>
 __device__ __forceinline__ void
-push_queue(PairQ& Q, const SolveParams<float>& P, F2 F0, const F2* DX, const F2* DY)
+push_queue(PairQ& Q, const PT& P, F2 F0, const F2* DX, const F2* DY)
 {
     if (XZ)
         zacc_push(Q.xa1, Q.xa2, Q.xa3, P.cxp[1], DX[0], DX[1], DX[2]);
@@ -454,9 +485,9 @@ push_queue(PairQ& Q, const SolveParams<float>& P, F2 F0, const F2* DX, const F2*
 // sum and difference, the xy diagonals and the z diagonals in packed lanes
 // (each stencil point one 8-byte load); the coefficient sums. Second
 // derivatives in difference form (below). F0 returns the pair's centre values.
-template <int BX, class FA, class FB>
+template <int BX, class FA, class FB, class PT>
 __device__ __forceinline__ void
-pair_derivs_q(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P,
+pair_derivs_q(const F2* __restrict__ c, const int* zo, const PT& P,
               PairQ& Q, FieldDerivs<float>& rA, FieldDerivs<float>& rB, F2& F0)
 {
     static_assert(FA::XY == FB::XY && FA::XZ == FB::XZ && FA::YZ == FB::YZ,
@@ -565,18 +596,18 @@ pair_derivs_q(const F2* __restrict__ c, const int* zo, const SolveParams<float>&
 #define ACB_D_AZ true, true, false, false, true, true
 #define ACB_D_SS true, true, true, false, false, false
 
-template <typename T>
+template <typename T, class PT>
 __device__ __forceinline__ void rhs_terms(const FieldDerivs<T>& lr, const FieldDerivs<T>& ux,
                                           const FieldDerivs<T>& uy, const FieldDerivs<T>& uz,
                                           const FieldDerivs<T>& ax, const FieldDerivs<T>& ay,
                                           const FieldDerivs<T>& az, const FieldDerivs<T>& ss,
-                                          const SolveParams<T>& P, T roc[ACB_NF], T cur[ACB_NF]);
+                                          const PT& P, T roc[ACB_NF], T cur[ACB_NF]);
 
 // Right-hand sides of the eight fields at one vertex, every stencil operand
 // read from the ring.
-template <typename T, int BX, int FIELD>
+template <typename T, int BX, int FIELD, class PT>
 __device__ __forceinline__ void
-mhd_rhs(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, T roc[ACB_NF],
+mhd_rhs(const state_t* __restrict__ c, const int* zo, const PT& P, T roc[ACB_NF],
         T cur[ACB_NF])
 {
     const auto lr = field_derivs<T, BX, ACB_D_LNRHO>(c + 0 * FIELD, zo, P);
@@ -593,9 +624,9 @@ mhd_rhs(const state_t* __restrict__ c, const int* zo, const SolveParams<T>& P, T
 // The same with the z register queues (single-precision stencils), one pair
 // array at a time: (lnrho, ss), (ux, ax), (uy, ay), (uz, az). cur2 returns the
 // centre values of each array.
-template <int BX, int FIELD>
+template <int BX, int FIELD, class PT>
 __device__ __forceinline__ void
-mhd_rhs_q(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P,
+mhd_rhs_q(const F2* __restrict__ c, const int* zo, const PT& P,
           float roc[ACB_NF], float cur[ACB_NF], F2 cur2[ACB_NARR], PairQ (&Q)[ACB_NARR])
 {
     FieldDerivs<float> lr, ux, uy, uz, ax, ay, az, ss;
@@ -610,9 +641,9 @@ mhd_rhs_q(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P,
     rhs_terms(lr, ux, uy, uz, ax, ay, az, ss, P, roc, cur);
 }
 
-template <int BX, int FIELD>
+template <int BX, int FIELD, class PT>
 __device__ __forceinline__ void
-prime_queues(const F2* __restrict__ c, const int* zo, const SolveParams<float>& P,
+prime_queues(const F2* __restrict__ c, const int* zo, const PT& P,
              PairQ (&Q)[ACB_NARR])
 {
     prime_pair<BX, false, false>(c + 0 * FIELD, zo, P, Q[0]);
@@ -623,11 +654,11 @@ prime_queues(const F2* __restrict__ c, const int* zo, const SolveParams<float>& 
 
 // Right-hand sides from the derivative sets (stencil_kernel.ac:355-528,
 // restated; same terms).
-template <typename T>
+template <typename T, class PT>
 __device__ __forceinline__ void
 rhs_terms(const FieldDerivs<T>& lr, const FieldDerivs<T>& ux, const FieldDerivs<T>& uy,
           const FieldDerivs<T>& uz, const FieldDerivs<T>& ax, const FieldDerivs<T>& ay,
-          const FieldDerivs<T>& az, const FieldDerivs<T>& ss, const SolveParams<T>& P,
+          const FieldDerivs<T>& az, const FieldDerivs<T>& ss, const PT& P,
           T roc[ACB_NF], T cur[ACB_NF])
 {
     cur[0] = lr.v;
@@ -865,9 +896,9 @@ member_of(const MemberDesc<T>* md, int n, long long t)
 // One task of a consumer warp: the planes of one (tile, z segment) column.
 // Waits for the ring, computes and stores every output plane, releases the
 // slots, and advances the plane counter q. Returns false if the CTA aborts.
-template <class Cfg, int STEP, bool ENS>
+template <class Cfg, int STEP, bool ENS, class PT>
 __device__ __forceinline__ bool
-consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<AcReal>& P,
+consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
              long long lt, state_t* out, float* in_lo, float* out_lo, const void* ring,
              uint64_t* full, uint64_t* empty, volatile int* abort_flag, uint32_t& q,
              const void* centre, uint64_t* full_c, uint64_t* empty_c, uint32_t& oq)
@@ -1088,9 +1119,13 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const SolveParams<
 // halo reads of each other's planes hit L2. With ENS the tasks of all members
 // of an ensemble form one list (member-major) and each task reads its member's
 // map, geometry, buffers and parameters from the descriptor table.
+template <bool ENS>
+using SolveKernelArgs = typename std::conditional<ENS, EnsSolveArgs<AcReal>, SolveArgs<AcReal>>::type;
+
 template <class Cfg, int STEP, bool ENS>
 __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
-    solve_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ SolveArgs<AcReal> a,
+    solve_kernel(const __grid_constant__ CUtensorMap tin,
+                 const __grid_constant__ SolveKernelArgs<ENS> a,
                  const __grid_constant__ CentreMaps cm)
 {
     using T = AcReal;
@@ -1111,7 +1146,6 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     __shared__ __align__(8) uint64_t empty_c[NCS];
     unsigned char* centre = smem_raw + Cfg::ring_bytes(); // NC slots of centre_slot_bytes
     __shared__ volatile int abort_flag;
-    __shared__ SolveParams<T> sP[CWARPS]; // ensemble: each consumer warp's copy of its member's parameters
 
     const int tid  = threadIdx.x;
     const int warp = tid >> 5;
@@ -1130,7 +1164,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     }
     __syncthreads();
 
-    const long long ntasks = ENS ? a.total_tasks : a.g.tasks;
+    const long long ntasks = ENS ? a.total_tasks : a.g.tasks; // (ENS: the group's tasks)
 
     if constexpr (Cfg::WGSPEC) {
         // whole warpgroups: warps 0..7 consume, warps 8..11 produce
@@ -1153,12 +1187,13 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
                 const CUtensorMap* map = &tin;
                 const SolveGeom* g     = &a.g;
                 long long lt           = t;
-                if (ENS) {
-                    const int m                = member_of(a.members, a.nmembers, t);
-                    const MemberDesc<T>* md    = a.members + m;
-                    map                        = &md->tmap;
-                    g                          = &md->g;
-                    lt                         = t - md->task_begin;
+                if constexpr (ENS) {
+                    const long long tg_      = t + a.task_base; // task in the whole list
+                    const int m              = member_of(a.members, a.nmembers, tg_);
+                    const MemberDesc<T>* md  = a.members + m;
+                    map                      = &md->tmap;
+                    g                        = &md->g;
+                    lt                       = tg_ - md->task_begin;
                     if (m != last_m) {
                         fence_tensormap_acquire(map);
                         prefetch_tensormap(map);
@@ -1230,17 +1265,13 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     for (long long t = blockIdx.x; t < ntasks; t += gridDim.x) {
         bool ok;
         if constexpr (ENS) {
-            const int m             = member_of(a.members, a.nmembers, t);
+            // the group's members: descriptor table and parameters from the
+            // launch (a.members points at the group's first descriptor)
+            const long long tg_     = t + a.task_base;
+            const int m             = member_of(a.members, a.nmembers, tg_);
             const MemberDesc<T>* md = a.members + m;
-            // each warp keeps its own copy, so no barrier across warps is needed
-            __syncwarp();
-            const int* srcw = reinterpret_cast<const int*>(&md->P);
-            int* dstw       = reinterpret_cast<int*>(&sP[warp]);
-            for (int w = lane; w < (int)(sizeof(SolveParams<T>) / sizeof(int)); w += 32)
-                dstw[w] = srcw[w];
-            __syncwarp();
-            const SolveGeom gv = md->g;
-            ok = consume_task<Cfg, STEP, ENS>(a, gv, sP[warp], t - md->task_begin, md->out,
+            const SolveGeom gv      = md->g;
+            ok = consume_task<Cfg, STEP, ENS>(a, gv, a.mp[m], tg_ - md->task_begin, md->out,
                                               md->in_lo, md->out_lo, ring, full, empty,
                                               &abort_flag, q, centre, full_c, empty_c, oq);
         }
