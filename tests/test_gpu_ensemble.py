@@ -112,3 +112,32 @@ def test_autotuner_keeps_state_and_caches(tmp_path):
         ens2.auto_optimize(cache)
         assert ens2.schedule() == chosen
     assert len(open(cache).read().split()) == 3
+
+
+def test_ensemble_larger_than_one_launch_group():
+    """An ensemble of more members than one launch carries parameters for (64)
+    runs in several launches per substep; every member must still equal its
+    mesh advanced alone, bit for bit."""
+    prec = abi.SP
+    sizes = [(8 + k % 5, 7 + k % 3, 6 + k % 4) for k in range(70)]
+    infos = [member_info(prec, n, k) for k, n in enumerate(sizes)]
+    fields = [member_fields(prec, n, k) for k, n in enumerate(sizes)]
+    with Ensemble("sp", infos) as ens:
+        for k in range(len(sizes)):
+            ens.load_member(k, abi.HostMesh(prec, infos[k], fields[k]))
+        ens.integrate_step(1e-3)
+        ens.synchronize()
+        assert ens.status() == 0
+        got = []
+        for k in range(len(sizes)):
+            h = abi.HostMesh(prec, infos[k])
+            ens.store_member(k, h)
+            got.append(h.fields)
+    for k in range(len(sizes)):  # members of both launch groups
+        host = abi.HostMesh(prec, infos[k], [f.copy() for f in fields[k]])
+        with Device("sp", infos[k]) as dev:
+            dev.load_mesh(host)
+            dev.integrate_step(1e-3)
+            dev.store_mesh(host)
+        for w in range(8):
+            assert np.array_equal(got[k][w], host.fields[w]), (k, w)
