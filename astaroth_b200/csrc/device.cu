@@ -309,6 +309,7 @@ acb_host::make_params(const AcMeshInfo& uniforms, const Layout& L, int step, int
     P.gamma_inv_cp = (AcReal)(gamma / cp);
     P.lnrho0       = rp[AC_lnrho0];
     P.lnT0         = rp[AC_lnT0];
+    P.exp_lnT0     = (AcReal)exp((double)rp[AC_lnT0]);
     P.k_heat       = (AcReal)0.001; // AC_THERMAL_CONDUCTIVITY of the module
 
     // Williamson (1980) 2N coefficients, "previous state" form

@@ -156,6 +156,7 @@ member_params(const SolveParams<AcReal>& P)
     m.gamma_inv_cp = P.gamma_inv_cp;
     m.lnrho0       = P.lnrho0;
     m.lnT0         = P.lnT0;
+    m.exp_lnT0     = P.exp_lnT0;
     m.k_heat       = P.k_heat;
     return m;
 }
