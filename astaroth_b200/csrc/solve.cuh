@@ -786,27 +786,17 @@ forcing_at(const SolveParams<T>& P, int i, int j, int k, T f[3])
         f[0] = f[1] = f[2] = 0;
 }
 
-// Compensated sum of the float pair (hi, lo) and a float increment d.
-__device__ __forceinline__ void
-pair_add(float hi, float lo, float d, float& ohi, float& olo)
-{
-    const float s  = hi + d;
-    const float bb = s - hi;
-    const float e  = (hi - (s - bb)) + (d - bb); // two-sum error
-    const float l  = lo + e;
-    ohi            = s + l; // renormalise
-    olo            = l - (ohi - s);
-}
-
-// pair_add of two fields in packed lanes (the same operations lane by lane).
+// Compensated sum of float pairs (hi, lo) and float increments d, two fields
+// in packed lanes: a two-sum of hi and d (s and its exact error e), the error
+// added to lo, and the result renormalised so that |olo| <= ulp(ohi) / 2.
 __device__ __forceinline__ void
 pair_add2(F2 hi, F2 lo, F2 d, F2& ohi, F2& olo)
 {
     const F2 s  = add2(hi, d);
     const F2 bb = sub2(s, hi);
-    const F2 e  = add2(sub2(hi, sub2(s, bb)), sub2(d, bb));
+    const F2 e  = add2(sub2(hi, sub2(s, bb)), sub2(d, bb)); // two-sum error
     const F2 l  = add2(lo, e);
-    ohi         = add2(s, l);
+    ohi         = add2(s, l); // renormalise
     olo         = sub2(l, sub2(ohi, s));
 }
 
@@ -1032,7 +1022,7 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
                 //          (hi, lo) = (cur, cur_lo) + d, a two-sum  [+ forcing]
                 // Forcing acts on ux, uy, uz, lane 0 of arrays 1-3; the lane of
                 // ax, ay, az adds 0 (for the mixed pair, adding 0 to a pair that
-                // pair_add returned leaves it as it is).
+                // pair_add2 returned leaves it as it is).
                 const acb::F2 rkA2 = acb::pk2(rkA, rkA), rkB2 = acb::pk2(rkB, rkB);
                 acb::F2* o2 = reinterpret_cast<acb::F2*>(out);
 #if ACB_MIXED
