@@ -1430,6 +1430,49 @@ acDeviceGetStatus(const Device device, unsigned* status)
 }
 
 AcResult
+acDeviceResetStatus(const Device device)
+{
+    cudaSetDevice(device->id);
+    ACB_CUDA_CHECK(cudaDeviceSynchronize());
+    ACB_CUDA_CHECK(cudaMemset(device->status, 0, sizeof(unsigned)));
+    return AC_SUCCESS;
+}
+
+// One warp waits, with the pipelines' bounded wait and a limit of limit_ns,
+// on phase 0 of an mbarrier that expects one arrival and gets none; when the
+// wait gives up, the warp raises the status bit a pipeline kernel raises and
+// the kernel returns.
+__global__ void
+wait_check_kernel(unsigned* status, unsigned long long limit_ns)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+    }
+    __syncwarp();
+    const bool ok = mbar_wait_limit(&bar, 0u, limit_ns);
+    if (!__all_sync(0xffffffffu, ok) && threadIdx.x == 0)
+        atomicOr(status, (unsigned)ACB_STATUS_TMA_TIMEOUT);
+}
+
+AcResult
+acDeviceCheckWaitLimit(const Device device, const double seconds)
+{
+    if (!(seconds > 0.0 && seconds <= 10.0))
+        return AC_FAILURE;
+    cudaSetDevice(device->id);
+    const cudaStream_t st = device->streams[STREAM_DEFAULT];
+    wait_check_kernel<<<1, 32, 0, st>>>(device->status, (unsigned long long)(seconds * 1e9));
+    ACB_CUDA_CHECK(cudaGetLastError());
+    device->launches++;
+    ACB_CUDA_CHECK(cudaStreamSynchronize(st));
+    unsigned s = 0;
+    ACB_CUDA_CHECK(cudaMemcpy(&s, device->status, sizeof(s), cudaMemcpyDeviceToHost));
+    return (s & ACB_STATUS_TMA_TIMEOUT) ? AC_SUCCESS : AC_FAILURE;
+}
+
+AcResult
 acDeviceGetCudaStream(const Device device, const Stream stream, void** cuda_stream)
 {
     *cuda_stream = (void*)stream_of(device, stream);

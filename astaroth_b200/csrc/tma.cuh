@@ -73,10 +73,10 @@ global_timer_ns()
     return t;
 }
 
-// Waits for the phase with the given parity to complete. Returns false if the
-// wall-clock limit ran out first.
+// Waits for the phase with the given parity to complete. Returns false if
+// limit_ns of wall time ran out first.
 __device__ __forceinline__ bool
-mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+mbar_wait_limit(uint64_t* bar, uint32_t parity, uint64_t limit_ns)
 {
     if (mbar_try_wait(bar, parity))
         return true;
@@ -84,9 +84,16 @@ mbar_wait_bounded(uint64_t* bar, uint32_t parity)
     for (uint32_t it = 0;; ++it) {
         if (mbar_try_wait(bar, parity))
             return true;
-        if ((it & 63u) == 63u && global_timer_ns() - t0 > ACB_WAIT_LIMIT_NS)
+        if ((it & 63u) == 63u && global_timer_ns() - t0 > limit_ns)
             return false;
     }
+}
+
+// The pipelines' wait: ACB_WAIT_LIMIT_NS.
+__device__ __forceinline__ bool
+mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+{
+    return mbar_wait_limit(bar, parity, ACB_WAIT_LIMIT_NS);
 }
 
 // 4-D tiled TMA load (x, y, z, field) into shared memory, completing on `bar`.

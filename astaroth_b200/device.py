@@ -166,6 +166,15 @@ class Device:
         _check(self.lib.acDeviceGetStatus(self.handle, C.byref(s)), "acDeviceGetStatus")
         return s.value
 
+    def reset_status(self) -> None:
+        _check(self.lib.acDeviceResetStatus(self.handle), "acDeviceResetStatus")
+
+    def check_wait_limit(self, seconds: float) -> None:
+        """acDeviceCheckWaitLimit: a bounded wait on a barrier nothing completes
+        must give up after `seconds` and raise status bit 0."""
+        _check(self.lib.acDeviceCheckWaitLimit(self.handle, float(seconds)),
+               "acDeviceCheckWaitLimit")
+
     def cuda_stream(self, stream: int = 0) -> int:
         p = C.c_void_p()
         _check(self.lib.acDeviceGetCudaStream(self.handle, stream, C.byref(p)),

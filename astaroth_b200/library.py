@@ -50,7 +50,8 @@ ASTAROTH_UTILS_H = [
     "acEvalError", "acVerifyMesh",
 ]
 ASTAROTH_B200_H = [
-    "acDeviceGetStatus", "acDeviceGetCudaStream", "acDeviceGetLaunchCount",
+    "acDeviceGetStatus", "acDeviceResetStatus", "acDeviceCheckWaitLimit",
+    "acDeviceGetCudaStream", "acDeviceGetLaunchCount",
     "acDeviceSetSolveConfig", "acDeviceGetSolveConfig", "acSolveConfigName",
     "acDeviceGetMemoryFootprint", "acDeviceIntegrateStep", "acDeviceIntegrateSteps",
     "acDeviceSetForcing", "acDeviceLoadVertexBufferDouble", "acDeviceStoreVertexBufferDouble",
@@ -150,6 +151,8 @@ def _declare(lib: C.CDLL, prec: abi.Precision) -> None:
         "acVerifyMesh": (res, [C.c_char_p, Mesh, Mesh]),
         # additions
         "acDeviceGetStatus": (res, [Dev, C.POINTER(C.c_uint)]),
+        "acDeviceResetStatus": (res, [Dev]),
+        "acDeviceCheckWaitLimit": (res, [Dev, C.c_double]),
         "acDeviceGetCudaStream": (res, [Dev, i, C.POINTER(C.c_void_p)]),
         "acDeviceGetLaunchCount": (res, [Dev, C.POINTER(C.c_ulonglong)]),
         "acDeviceSetSolveConfig": (res, [Dev, i]),

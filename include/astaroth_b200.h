@@ -18,6 +18,18 @@ extern "C" {
  * synchronises the device. */
 AcResult acDeviceGetStatus(const Device device, unsigned* status);
 
+/* Clears the status word (after the caller has dealt with a reported
+ * failure; the device and its buffers stay usable). Synchronises. */
+AcResult acDeviceResetStatus(const Device device);
+
+/* Exercises the failure path of the bounded waits: launches one kernel that
+ * waits, with the same bounded wait the solve pipeline uses but a limit of
+ * `seconds`, on a barrier phase that nothing completes. The wait gives up,
+ * the kernel raises status bit 0 and returns, as a pipeline kernel whose
+ * copies never arrived would. Synchronises; returns AC_SUCCESS when the
+ * status bit was raised and the device still answers. */
+AcResult acDeviceCheckWaitLimit(const Device device, const double seconds);
+
 /* The CUDA stream (cudaStream_t) behind a Stream handle, so a caller can
  * order its own work or CUDA events with the device's. */
 AcResult acDeviceGetCudaStream(const Device device, const Stream stream, void** cuda_stream);

@@ -645,3 +645,38 @@ def test_staged_loads(flavour):
         dev.store_mesh(back)
         for w in range(8):
             assert np.array_equal(back.fields[w], fields[w]), w
+
+
+def test_bounded_wait_gives_up_and_device_stays_usable():
+    """Failure detection without a fault: a kernel waits, with the solve
+    pipeline's bounded wait and a 0.2 s limit, on a barrier phase that nothing
+    completes. The wait gives up, the status word reports it, a whole-device
+    synchronisation returns AC_FAILURE, and after the status is reset the same
+    Device integrates exactly as a fresh one does."""
+    import time
+
+    from astaroth_b200.device import AcError
+
+    prec = abi.PRECISIONS["sp"]
+    n = 16
+    info = workload_info(prec, n)
+    fields = init.workload_fields(n, n, n, prec.np_dtype, seed=23, amplitude=1e-3)
+    with new_device("sp", info) as dev:
+        assert dev.status() == 0
+        t0 = time.perf_counter()
+        dev.check_wait_limit(0.2)
+        waited = time.perf_counter() - t0
+        assert 0.2 <= waited < 5.0
+        assert dev.status() == 1
+        with pytest.raises(AcError):
+            dev.synchronize()
+        dev.reset_status()
+        assert dev.status() == 0
+        dev.load_mesh(abi.HostMesh(prec, info, [f.copy() for f in fields]))
+        dev.integrate_step(1e-3)
+        dev.synchronize()
+        assert dev.status() == 0
+        got = [dev.store_double(w) for w in range(8)]
+    ref = run_gpu("sp", fields, info, 1e-3, 1)
+    for w in range(8):
+        assert np.array_equal(interior(got[w]), interior(ref[w])), w
