@@ -1,0 +1,53 @@
+"""The JSON line of bench.py: the reference arm (the reference's own host
+solver, or the oracle port where that build is absent) runs on the CPU and
+prints the contract's keys; the byte accounting and the figures read from the
+committed files are the ones the GPU arm reports."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.join(HERE, "..")
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+
+def test_reference_arm_prints_the_contract_line():
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1",
+                        "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    assert d["unit"] == "cell-updates/s" and d["higher_is_better"] is True
+    assert d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 1 and d["n_gpus"] == 1
+    assert d["config"]["workload"].startswith("MHD RK3, 512^3")
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["sample"]
+    assert cb["value"] == pytest.approx(d["value"])
+    e = d["e2e"]
+    assert e["value"] == pytest.approx(d["value"]) and e["unit"] == d["unit"]
+    assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+
+
+def test_algorithmic_bytes_per_step():
+    # s = 0 reads in and writes out; s = 1, 2 read in and out and write out:
+    # 8 array touches of 8 fields per step
+    n = 512
+    assert bench.alg_bytes_per_step("sp", n) == 8 * 4 * 8 * n ** 3
+    assert bench.alg_bytes_per_step("mixed", n) == 8 * 8 * 8 * n ** 3
+    assert bench.alg_bytes_per_step("dp", n) == bench.alg_bytes_per_step("mixed", n)
+
+
+def test_traffic_and_peak_come_from_committed_files():
+    t = bench.profile_traffic("solve_mixed_256.md")
+    # a 512^3 s = 1 launch moves about 192 B per cell (hi and lo of in, out read,
+    # out written); the committed capture is within 10 % of that
+    assert t is not None and abs(t / (192 * 512 ** 3) - 1.0) < 0.10
+    peak, kind = bench.measured_peak_hbm()
+    assert kind == "measured" and 5000.0 < peak < 8000.0
