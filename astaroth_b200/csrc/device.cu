@@ -77,11 +77,25 @@ struct device_s {
     CentreMaps cmap[2]; // by parity of `in`: centre boxes over out hi, in lo, out lo
     int tmap_cfg;       // configuration the maps were encoded for (-1: none)
 
-    double* red_partials;
+    double* red_partials; // 3 * red_max_blocks (the three-in-one pass)
     int red_max_blocks;
     unsigned* red_counter;
-    double* red_result;
-    double* h_result; // pinned
+    double* red_result; // 3 doubles
+    double* h_result;   // pinned, 3 doubles
+    // Interiors written so far: bumped by every operation that can change a
+    // block's interior values (the solve, loads, fills of whole fields,
+    // transfers, graph replays). A MAX / MIN / RMS reduction of one field or
+    // one vector's length computes all three in one pass (reduce3_kernel) and
+    // keeps them here with the block and the epoch they were taken at; the
+    // other two then come from this record while nothing has changed.
+    unsigned long long write_epoch;
+    struct {
+        bool valid;
+        const void* block;
+        unsigned long long epoch;
+        int nin, handles[3];
+        double vals[3]; // MAX, MIN, RMS sum
+    } red3;
 
     double* xfer; // device staging buffer for the double-precision views
     size_t xfer_elems;
@@ -429,6 +443,7 @@ launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e)
     kern<<<(unsigned)grid, cfg.threads, cfg.smem, st>>>(d->tmap[d->cur], a, d->cmap[d->cur]);
     ACB_CUDA_CHECK(cudaGetLastError());
     d->launches++;
+    d->write_epoch++;
     d->ghost_ok[d->cur ^ 1] = false; // the out block's ghosts are stale now
     d->lo_stale[d->cur ^ 1] = false; // (all of them, hi and lo alike)
     return AC_SUCCESS;
@@ -525,6 +540,34 @@ run_reduce(const Device d, cudaStream_t st, int rtype, int nin, const int* handl
     a.result   = d->red_result;
     long long blocks = (a.rows + 7) / 8;
     blocks           = std::max(1LL, std::min(blocks, (long long)d->red_max_blocks));
+    const int which  = rtype == RTYPE_MAX ? 0 : (rtype == RTYPE_MIN ? 1 : (rtype == RTYPE_RMS ? 2 : -1));
+    if (which >= 0 && (nin == RED_SCAL || nin == RED_VEC)) {
+        // MAX, MIN and RMS together: one pass over the fields serves all three
+        // requests while the block is unchanged (the diagnostics of a step)
+        auto& c        = d->red3;
+        const bool hit = c.valid && c.block == d->blk[d->cur] && c.epoch == d->write_epoch &&
+                         c.nin == nin && c.handles[0] == handles[0] &&
+                         (nin == RED_SCAL ||
+                          (c.handles[1] == handles[1] && c.handles[2] == handles[2]));
+        if (!hit) {
+            reduce3_kernel<256><<<(unsigned)blocks, 256, 0, st>>>(a);
+            ACB_CUDA_CHECK(cudaGetLastError());
+            d->launches++;
+            ACB_CUDA_CHECK(cudaMemcpyAsync(d->h_result, d->red_result, 3 * sizeof(double),
+                                           cudaMemcpyDeviceToHost, st));
+            ACB_CUDA_CHECK(cudaStreamSynchronize(st));
+            c.valid = true;
+            c.block = d->blk[d->cur];
+            c.epoch = d->write_epoch;
+            c.nin   = nin;
+            for (int w = 0; w < 3; ++w) {
+                c.handles[w] = w < nin ? handles[w] : -1;
+                c.vals[w]    = d->h_result[w];
+            }
+        }
+        *result = c.vals[which];
+        return AC_SUCCESS;
+    }
     reduce_kernel<256><<<(unsigned)blocks, 256, 0, st>>>(a);
     ACB_CUDA_CHECK(cudaGetLastError());
     d->launches++;
@@ -682,6 +725,8 @@ launch_pack(const Device d, cudaStream_t st, int blk, int handle, double* flat, 
     pack_kernel<<<d->num_sms * 8, 256, 0, st>>>(L, f, lo, flat, to_flat, fill, value);
     ACB_CUDA_CHECK(cudaGetLastError());
     d->launches++;
+    if (!to_flat)
+        d->write_epoch++;
     return AC_SUCCESS;
 }
 
@@ -926,11 +971,11 @@ acDeviceCreate(const int id, const AcMeshInfo config, Device* device_handle)
 #endif
     }
     d->red_max_blocks = d->num_sms * 8;
-    ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_partials, sizeof(double) * d->red_max_blocks));
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_partials, 3 * sizeof(double) * d->red_max_blocks));
     ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_counter, sizeof(unsigned)));
     ACB_CUDA_CHECK(cudaMemset(d->red_counter, 0, sizeof(unsigned)));
-    ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_result, sizeof(double)));
-    ACB_CUDA_CHECK(cudaMallocHost((void**)&d->h_result, sizeof(double)));
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_result, 3 * sizeof(double)));
+    ACB_CUDA_CHECK(cudaMallocHost((void**)&d->h_result, 3 * sizeof(double)));
     ACB_CUDA_CHECK(cudaMalloc((void**)&d->status, sizeof(unsigned)));
     ACB_CUDA_CHECK(cudaMemset(d->status, 0, sizeof(unsigned)));
     if (stage_create(&d->stage, (size_t)d->L.mx * d->L.my * d->L.mz) != AC_SUCCESS)
@@ -1020,6 +1065,7 @@ acDeviceAutoOptimize(const Device device)
         }
     }
     device->solve_cfg = best;
+    device->write_epoch++;
     ACB_CUDA_CHECK(cudaMemcpyAsync(device->blk[device->cur ^ 1], save, bytes,
                                    cudaMemcpyDeviceToDevice, st));
     device->ghost_ok[device->cur ^ 1] = false;
@@ -1052,6 +1098,7 @@ acDeviceLoadVertexBufferWithOffset(const Device device, const Stream stream,
     const Layout& L   = device->L;
     float* lo         = device->lo[device->cur] ? device->lo[device->cur] + fidx(L, h, 0) : nullptr;
     device->ghost_ok[device->cur] = false;
+    device->write_epoch++;
     if (ensure_lo_ghosts(device, stream_of(device, stream), device->cur) != AC_SUCCESS)
         return AC_FAILURE;
     return copy_field_range(stream_of(device, stream), L,
@@ -1192,6 +1239,7 @@ acDeviceTransferVertexBufferWithOffset(const Device src_device, const Stream str
     }
     cudaSetDevice(src_device->id);
     dst_device->ghost_ok[dst_device->cur] = false;
+    dst_device->write_epoch++;
     const cudaStream_t tst = stream_of(src_device, stream);
     if (ensure_lo_ghosts(src_device, tst, src_device->cur) != AC_SUCCESS ||
         ensure_lo_ghosts(dst_device, tst, dst_device->cur) != AC_SUCCESS)
@@ -1627,6 +1675,7 @@ acDeviceIntegrateSteps(const Device device, const Stream stream, const AcReal dt
             device->graph_key[p] = key;
         }
         ACB_CUDA_CHECK(cudaGraphLaunch(device->graph[p], st));
+        device->write_epoch++; // the replayed solves wrote both blocks
         device->launches += device->graph_launches[p];
         device->ghost_ok[0] = device->graph_ghost[p][0]; // as the captured step left them
         device->ghost_ok[1] = device->graph_ghost[p][1];

@@ -66,6 +66,15 @@ red_load(const ReduceArgs& a, int w, long long id)
     return v;
 }
 
+// |v|^2 of a vector, with one fixed rounding sequence for every reduction
+// that uses it (the length for MAX / MIN, the square for RMS), so that a pass
+// computing several of them returns what separate passes return, bit for bit.
+__device__ __forceinline__ double
+red_len2(double x, double y, double z)
+{
+    return __fma_rn(z, z, __fma_rn(y, y, __dmul_rn(x, x)));
+}
+
 __device__ __forceinline__ double
 red_filter(const ReduceArgs& a, long long id)
 {
@@ -73,7 +82,7 @@ red_filter(const ReduceArgs& a, long long id)
     if (a.nin == RED_SCAL) {
         const double v = red_load(a, 0, id);
         if (rt == RTYPE_RMS)
-            return v * v;
+            return __dmul_rn(v, v);
         if (rt == RTYPE_RMS_EXP) {
             const double e = exp(v);
             return e * e;
@@ -83,12 +92,12 @@ red_filter(const ReduceArgs& a, long long id)
     const double x = red_load(a, 0, id), y = red_load(a, 1, id), z = red_load(a, 2, id);
     if (a.nin == RED_VEC) {
         if (rt == RTYPE_RMS)
-            return x * x + y * y + z * z;
+            return red_len2(x, y, z);
         if (rt == RTYPE_RMS_EXP) {
             const double ex = exp(x), ey = exp(y), ez = exp(z);
             return ex * ex + ey * ey + ez * ez;
         }
-        return sqrt(x * x + y * y + z * z); // MAX, MIN, SUM of the length
+        return sqrt(red_len2(x, y, z)); // MAX, MIN, SUM of the length
     }
     // Alfven speed with density exponent d
     const double d  = red_load(a, 3, id);
@@ -154,6 +163,109 @@ reduce_kernel(const ReduceArgs a)
                 b = red_combine(a.rtype, b, wsum[w]);
             *a.result  = b;
             *a.counter = 0u; // ready for the next launch on this stream
+        }
+    }
+}
+
+// MAX, MIN and the RMS sum of one scalar field or one vector's length in a
+// single pass (a.rtype unused): three accumulators, each combined in exactly
+// the order reduce_kernel combines its one, so result[0..2] equal the MAX,
+// MIN and RMS passes' results bit for bit. partials holds 3 * gridDim.x.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS)
+reduce3_kernel(const ReduceArgs a)
+{
+    const Layout& L = a.L;
+    const int lane  = threadIdx.x & 31;
+    const int wid   = threadIdx.x >> 5;
+    const long long gw  = ((long long)blockIdx.x * THREADS + threadIdx.x) >> 5;
+    const long long nw  = ((long long)gridDim.x * THREADS) >> 5;
+    const int rx        = a.end.x - a.start.x;
+    const int ry        = a.end.y - a.start.y;
+    double mx = -INFINITY, mn = INFINITY, sm = 0.0;
+    for (long long r = gw; r < a.rows; r += nw) {
+        const int j          = a.start.y + (int)(r % ry);
+        const int k          = a.start.z + (int)(r / ry);
+        const long long base = lidx(L, a.start.x, j, k);
+        for (int i = lane; i < rx; i += 32) {
+            const long long id = base + i;
+            double m, q;
+            if (a.nin == RED_SCAL) {
+                m = red_load(a, 0, id);
+                q = __dmul_rn(m, m);
+            }
+            else {
+                q = red_len2(red_load(a, 0, id), red_load(a, 1, id), red_load(a, 2, id));
+                m = sqrt(q);
+            }
+            mx = fmax(mx, m);
+            mn = fmin(mn, m);
+            sm = sm + q;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        sm = sm + __shfl_xor_sync(0xffffffffu, sm, o);
+    }
+    __shared__ double wmx[THREADS / 32], wmn[THREADS / 32], wsm[THREADS / 32];
+    __shared__ bool last;
+    if (lane == 0) {
+        wmx[wid] = mx;
+        wmn[wid] = mn;
+        wsm[wid] = sm;
+    }
+    __syncthreads();
+    const unsigned G = gridDim.x;
+    if (threadIdx.x == 0) {
+        double bx = wmx[0], bn = wmn[0], bs = wsm[0];
+        for (int w = 1; w < THREADS / 32; ++w) {
+            bx = fmax(bx, wmx[w]);
+            bn = fmin(bn, wmn[w]);
+            bs = bs + wsm[w];
+        }
+        a.partials[blockIdx.x]         = bx;
+        a.partials[G + blockIdx.x]     = bn;
+        a.partials[2 * G + blockIdx.x] = bs;
+        __threadfence();
+        const unsigned done = atomicAdd(a.counter, 1u);
+        last                = (done == G - 1);
+    }
+    __syncthreads();
+    if (last) {
+        // the fixed-order fold of reduce_kernel, for each accumulator
+        __threadfence();
+        const volatile double* P = a.partials;
+        double vx = -INFINITY, vn = INFINITY, vs = 0.0;
+        for (int b = threadIdx.x; b < (int)G; b += THREADS) {
+            vx = fmax(vx, P[b]);
+            vn = fmin(vn, P[G + b]);
+            vs = vs + P[2 * G + b];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            vx = fmax(vx, __shfl_xor_sync(0xffffffffu, vx, o));
+            vn = fmin(vn, __shfl_xor_sync(0xffffffffu, vn, o));
+            vs = vs + __shfl_xor_sync(0xffffffffu, vs, o);
+        }
+        if (lane == 0) {
+            wmx[wid] = vx;
+            wmn[wid] = vn;
+            wsm[wid] = vs;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double bx = wmx[0], bn = wmn[0], bs = wsm[0];
+            for (int w = 1; w < THREADS / 32; ++w) {
+                bx = fmax(bx, wmx[w]);
+                bn = fmin(bn, wmn[w]);
+                bs = bs + wsm[w];
+            }
+            a.result[0] = bx;
+            a.result[1] = bn;
+            a.result[2] = bs;
+            *a.counter  = 0u; // ready for the next launch on this stream
         }
     }
 }

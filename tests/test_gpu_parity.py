@@ -680,3 +680,63 @@ def test_bounded_wait_gives_up_and_device_stays_usable():
     ref = run_gpu("sp", fields, info, 1e-3, 1)
     for w in range(8):
         assert np.array_equal(interior(got[w]), interior(ref[w])), w
+
+
+@pytest.mark.parametrize("flavour", FLAVOURS)
+def test_reduction_record_follows_every_write(flavour):
+    """MAX, MIN and RMS of one field or of a vector's length come from one pass
+    and are kept while nothing has written the device's blocks; a step, a
+    fill, a load and a transfer must each make the next request read the new
+    values: device A (which holds a record) must return what device B (which
+    reduces the same state for the first time) returns."""
+    prec = abi.PRECISIONS[flavour]
+    n = 24
+    info = workload_info(prec, n)
+    f1 = init.workload_fields(n, n, n, prec.np_dtype, seed=31, amplitude=0.05)
+    f2 = init.workload_fields(n, n, n, prec.np_dtype, seed=32, amplitude=0.07)
+    U = (abi.VTXBUF_UUX, abi.VTXBUF_UUY, abi.VTXBUF_UUZ)
+    kinds = (abi.RTYPE_MAX, abi.RTYPE_MIN, abi.RTYPE_RMS)
+
+    def stats(dev):
+        v = [dev.reduce_vec_double(r, *U) for r in kinds]
+        s = [dev.reduce_scal_double(r, abi.VTXBUF_LNRHO) for r in kinds]
+        # asked again: the same values
+        assert [dev.reduce_vec_double(r, *U) for r in kinds] == v
+        return v + s
+
+    def fresh(setup):
+        with new_device(flavour, info) as b:
+            setup(b)
+            return stats(b)
+
+    with new_device(flavour, info) as a:
+        a.load_mesh(abi.HostMesh(prec, info, [f.copy() for f in f1]))
+        s0 = stats(a)
+        assert s0 == fresh(lambda b: b.load_mesh(abi.HostMesh(prec, info, [f.copy() for f in f1])))
+
+        a.integrate_step(1e-3)
+        s1 = stats(a)
+        assert s1 != s0
+
+        def stepped(b):
+            b.load_mesh(abi.HostMesh(prec, info, [f.copy() for f in f1]))
+            b.integrate_step(1e-3)
+        assert s1 == fresh(stepped)
+
+        a.set_vertex_buffer(abi.VTXBUF_UUX, 0.25)
+        s2 = stats(a)
+
+        def filled(b):
+            stepped(b)
+            b.set_vertex_buffer(abi.VTXBUF_UUX, 0.25)
+        assert s2 == fresh(filled)
+
+        a.load_mesh(abi.HostMesh(prec, info, [f.copy() for f in f2]))
+        assert stats(a) == fresh(lambda b: b.load_mesh(abi.HostMesh(prec, info, [f.copy() for f in f2])))
+
+        with new_device(flavour, info) as c:
+            c.load_mesh(abi.HostMesh(prec, info, [f.copy() for f in f1]))
+            rc = c.lib.acDeviceTransferMesh(c.handle, 0, a.handle)
+            assert rc == 0
+            c.synchronize()
+            assert stats(a) == s0
