@@ -716,8 +716,10 @@ def run_ours(args) -> None:
         torch.cuda.empty_cache()
         forced = forced_run(args.forced_n, min(args.steps, 20), max(args.warmup, 3), ranks, gpu)
 
+    # the reference host solver's baseline: one process on the host cores, so
+    # only in a one-GPU run (a multi-rank run reports none)
     cpu = None
-    if ranks.rank == 0 and not args.no_cpu:
+    if ranks.world == 1 and not args.no_cpu:
         c = cpu_reference_sample(budget_s=12.0)
         cpu = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
