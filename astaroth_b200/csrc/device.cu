@@ -53,6 +53,18 @@ acb_host::solve_configs(int* n)
 // ---------------------------------------------------------------------------
 // The device object
 // ---------------------------------------------------------------------------
+// One captured whole step and the host-side block state a replay leaves.
+struct StepGraph {
+    cudaGraphExec_t exec;
+    unsigned long long key;
+    double extra; // a launch parameter the graph was captured with (CFL: time scale)
+    unsigned long long launches;
+    bool ghost[2]; // ghost_ok of both blocks after a replay
+    bool lo[2];    // lo_stale of both blocks after a replay
+};
+
+enum { STEP_FIXED = 0, STEP_CFL = 1 };
+
 struct device_s {
     int id;
     AcMeshInfo local_config;
@@ -107,12 +119,14 @@ struct device_s {
     unsigned long long launches;
     unsigned long long uniform_version;
 
-    // whole-step graphs, one per starting buffer parity
-    cudaGraphExec_t graph[2];
-    unsigned long long graph_key[2];
-    unsigned long long graph_launches[2];
-    bool graph_ghost[2][2]; // ghost_ok of both blocks after a replay of graph[p]
-    bool graph_lo[2][2];    // lo_stale of both blocks after a replay of graph[p]
+    // whole-step graphs: [kind][starting buffer parity], kind 0 steps with
+    // the time step given by the caller, kind 1 with the time step chosen on
+    // the device (STEP_CFL)
+    StepGraph graph[2][2];
+
+    // time-step record of the steps whose dt is chosen on the device
+    // (device memory): dt of the last such step, simulated time, steps taken
+    double* cfl;
 };
 
 // ---------------------------------------------------------------------------
@@ -235,16 +249,17 @@ AcResult
 acb_host::prepare_table(const SolveConfig* cfgs, int n)
 {
     for (int c = 0; c < n; ++c)
-        for (int st = 0; st < 4; ++st) {
-            if (!cfgs[c].kern[st])
+        for (int st = 0; st < 7; ++st) {
+            // kern[0..3], then kern_dt[0..2]
+            const void* k = st < 4 ? cfgs[c].kern[st] : cfgs[c].kern_dt[st - 4];
+            if (!k)
                 continue;
-            ACB_CUDA_CHECK(cudaFuncSetAttribute((const void*)cfgs[c].kern[st],
-                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+            ACB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int)cfgs[c].smem));
             // kernels that move registers between warpgroups must start with
             // enough of them, or the consumers' increase would wait for ever
             cudaFuncAttributes fa;
-            ACB_CUDA_CHECK(cudaFuncGetAttributes(&fa, (const void*)cfgs[c].kern[st]));
+            ACB_CUDA_CHECK(cudaFuncGetAttributes(&fa, k));
             if (fa.numRegs < cfgs[c].launch_regs) {
                 fprintf(stderr,
                         "astaroth_b200: solve kernel %s built with %d registers a thread, "
@@ -269,6 +284,9 @@ prepare_kernels_once()
     done = true;
     return AC_SUCCESS;
 }
+
+// beta of the Williamson (1980) 2N scheme: rkB = beta[s] dt
+static const double kRkBeta[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
 
 // Kernel arguments from the uniform mirror (coefficients pre-scaled in double,
 // rounded once to AcReal).
@@ -328,7 +346,7 @@ acb_host::make_params(const AcMeshInfo& uniforms, const Layout& L, int step, int
 
     // Williamson (1980) 2N coefficients, "previous state" form
     const double alpha[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
-    const double beta[3]  = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+    const double* beta    = kRkBeta;
     const double dt       = rp[AC_dt];
     P.rkB                 = (AcReal)(beta[step] * dt);
     P.rkA                 = step > 0 ? (AcReal)(beta[step] * alpha[step] / beta[step - 1]) : 0;
@@ -392,8 +410,11 @@ box_in_interior(const Device d, int3 s, int3 e)
            e.y <= NGHOST + L.ny && e.z <= NGHOST + L.nz;
 }
 
+// dt_dev: when given, the solve reads the time step from this device double
+// (the record of acDeviceIntegrateStepCFL) instead of the AC_dt uniform.
 static AcResult
-launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e)
+launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e,
+             const double* dt_dev = nullptr)
 {
     if (step < 0 || step > 2) {
         fprintf(stderr, "astaroth_b200: invalid substep %d\n", step);
@@ -425,8 +446,13 @@ launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e)
     a.out_lo     = d->lo[d->cur ^ 1];
     a.status     = d->status;
     a.P          = make_params(d->uniforms, d->L, step, d->forcing);
+    if (dt_dev) {
+        a.P.dt_dev  = dt_dev;
+        a.P.rk_beta = kRkBeta[step];
+    }
 
-    const SolveKernelFn kern = (SolveKernelFn)cfg.kern[step == 2 && d->forcing ? 3 : step];
+    const SolveKernelFn kern = dt_dev ? (SolveKernelFn)cfg.kern_dt[step]
+                                      : (SolveKernelFn)cfg.kern[step == 2 && d->forcing ? 3 : step];
     int per_sm = 0;
     ACB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern,
                                                                  cfg.threads, cfg.smem));
@@ -516,12 +542,13 @@ launch_halo(const Device d, cudaStream_t st, int3 s, int3 e, int f0, int f1)
     return AC_SUCCESS;
 }
 
+// Arguments and grid of a reduction over the interior of the current block
+// into the Device's scratch (result in d->red_result).
 static AcResult
-run_reduce(const Device d, cudaStream_t st, int rtype, int nin, const int* handles,
-           double* result)
+reduce_args(const Device d, int rtype, int nin, const int* handles, ReduceArgs& a,
+            long long& blocks)
 {
     const Layout& L = d->L;
-    ReduceArgs a;
     memset(&a, 0, sizeof(a));
     a.L = L;
     for (int w = 0; w < nin; ++w) {
@@ -538,8 +565,19 @@ run_reduce(const Device d, cudaStream_t st, int rtype, int nin, const int* handl
     a.partials = d->red_partials;
     a.counter  = d->red_counter;
     a.result   = d->red_result;
-    long long blocks = (a.rows + 7) / 8;
-    blocks           = std::max(1LL, std::min(blocks, (long long)d->red_max_blocks));
+    blocks     = (a.rows + 7) / 8;
+    blocks     = std::max(1LL, std::min(blocks, (long long)d->red_max_blocks));
+    return AC_SUCCESS;
+}
+
+static AcResult
+run_reduce(const Device d, cudaStream_t st, int rtype, int nin, const int* handles,
+           double* result)
+{
+    ReduceArgs a;
+    long long blocks;
+    if (reduce_args(d, rtype, nin, handles, a, blocks) != AC_SUCCESS)
+        return AC_FAILURE;
     const int which  = rtype == RTYPE_MAX ? 0 : (rtype == RTYPE_MIN ? 1 : (rtype == RTYPE_RMS ? 2 : -1));
     if (which >= 0 && (nin == RED_SCAL || nin == RED_VEC)) {
         // MAX, MIN and RMS together: one pass over the fields serves all three
@@ -747,12 +785,157 @@ ensure_xfer(const Device d)
 static void
 invalidate_graphs(const Device d)
 {
-    for (int p = 0; p < 2; ++p) {
-        if (d->graph[p])
-            cudaGraphExecDestroy(d->graph[p]);
-        d->graph[p]     = nullptr;
-        d->graph_key[p] = 0;
+    for (int k = 0; k < 2; ++k)
+        for (int p = 0; p < 2; ++p) {
+            StepGraph& g = d->graph[k][p];
+            if (g.exec)
+                cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+            g.key  = 0;
+        }
+}
+
+// Replays num_steps whole steps of one kind from CUDA graphs, one per
+// starting buffer parity, capturing a graph (enqueue) when none matches the
+// key; the Device's host-side block state follows what the captured step left.
+template <class F>
+static AcResult
+replay_steps(const Device device, cudaStream_t st, int kind, unsigned long long base,
+             double extra, int num_steps, F enqueue)
+{
+    for (int i = 0; i < num_steps; ++i) {
+        const int p  = device->cur;
+        StepGraph& G = device->graph[kind][p];
+        // a captured step contains the ghost fill only when the ghosts were stale
+        const unsigned long long key = base ^ (device->ghost_ok[p] ? 2ull : 0ull);
+        if (!G.exec || G.key != key || G.extra != extra) {
+            if (G.exec)
+                cudaGraphExecDestroy(G.exec);
+            G.exec = nullptr;
+            cudaGraph_t g;
+            ACB_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            const unsigned long long before = device->launches;
+            const AcResult rc               = enqueue(device, st);
+            ACB_CUDA_CHECK(cudaStreamEndCapture(st, &g));
+            device->cur = p; // capture advanced the roles; replay does it below
+            G.launches  = device->launches - before;
+            G.ghost[0]  = device->ghost_ok[0];
+            G.ghost[1]  = device->ghost_ok[1];
+            G.lo[0]     = device->lo_stale[0];
+            G.lo[1]     = device->lo_stale[1];
+            device->launches = before;
+            if (rc != AC_SUCCESS) {
+                cudaGraphDestroy(g);
+                return AC_FAILURE;
+            }
+            ACB_CUDA_CHECK(cudaGraphInstantiate(&G.exec, g, 0));
+            cudaGraphDestroy(g);
+            G.key   = key;
+            G.extra = extra;
+        }
+        ACB_CUDA_CHECK(cudaGraphLaunch(G.exec, st));
+        device->write_epoch++; // the replayed solves wrote both blocks
+        device->launches += G.launches;
+        device->ghost_ok[0] = G.ghost[0]; // as the captured step left them
+        device->ghost_ok[1] = G.ghost[1];
+        device->lo_stale[0] = G.lo[0];
+        device->lo_stale[1] = G.lo[1];
+        device->cur ^= 1; // three swaps per step
     }
+    return AC_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Time step chosen on the device
+// ---------------------------------------------------------------------------
+// The reference standalone's loop picks each step's dt on the host
+// (samples/standalone/simulation.cc:429-436 with LSINK = LBFIELD = 0;
+// model/host_timestep.cc:33-60): a synchronising max |u| reduction, then
+//   uu_dt   = cdt dsmin / (|umax| + sqrt(cs2_sound))
+//   visc_dt = cdtv dsmin^2 / max(max(nu, eta), max(gamma, chi = 0))
+//   dt      = (AcReal)timescale * (AcReal)min(uu_dt, visc_dt)
+// Here the same formula runs in one GPU thread on the max |u| that
+// reduce3_kernel left in device memory, in double precision (the reference
+// host code uses long double), with umax first rounded to AcReal as the
+// reference's acReduceVec returns it. Nothing returns to the host, so a whole
+// simulation step, time step included, is one CUDA graph.
+struct CflParams {
+    double cdt, cdtv, dsmin, cs2, nu, eta, gamma;
+    AcReal timescale;
+};
+
+// rec: dt of the last step, simulated time, steps taken
+static __global__ void
+cfl_kernel(const double* umax, double* rec, const CflParams p)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    const double u       = (double)(AcReal)umax[0];
+    const double uu_dt   = p.cdt * p.dsmin / (fabs(u) + sqrt(p.cs2));
+    const double visc_dt = p.cdtv * p.dsmin * p.dsmin / fmax(fmax(p.nu, p.eta), fmax(p.gamma, 0.0));
+    const AcReal dt      = p.timescale * (AcReal)fmin(uu_dt, visc_dt);
+    rec[0]               = (double)dt;
+    rec[1] += (double)dt;
+    rec[2] += 1.0;
+}
+
+// The formula's parameters from the uniform mirror. AC_dsmin as the
+// standalone's config loader sets it (min of AC_dsx, AC_dsy, AC_dsz) where the
+// caller left it unset; AC_cdt and AC_cdtv must be positive.
+static AcResult
+cfl_params(const Device d, AcReal timescale, CflParams& cp)
+{
+    const AcReal* rp = d->uniforms.real_params;
+    cp.cdt           = rp[AC_cdt];
+    cp.cdtv          = rp[AC_cdtv];
+    cp.dsmin         = rp[AC_dsmin] > 0
+                           ? (double)rp[AC_dsmin]
+                           : (double)std::min(rp[AC_dsx], std::min(rp[AC_dsy], rp[AC_dsz]));
+    cp.cs2           = rp[AC_cs2_sound];
+    cp.nu            = rp[AC_nu_visc];
+    cp.eta           = rp[AC_eta];
+    cp.gamma         = rp[AC_gamma];
+    cp.timescale     = timescale;
+    if (!(cp.cdt > 0) || !(cp.cdtv > 0) || !(cp.dsmin > 0) || !(timescale > 0)) {
+        fprintf(stderr, "astaroth_b200: a time step chosen on the device needs AC_cdt, AC_cdtv, "
+                        "the grid spacings and the time scale positive\n");
+        return AC_FAILURE;
+    }
+    if (d->forcing) {
+        fprintf(stderr, "astaroth_b200: forcing scales with sqrt(dt) on the host; it does not "
+                        "combine with a time step chosen on the device\n");
+        return AC_FAILURE;
+    }
+    return AC_SUCCESS;
+}
+
+// max |u| into d->red_result, the time step into d->cfl, then the three
+// substeps reading it: 3 x (ghost fill, solve, swap).
+static AcResult
+enqueue_step_cfl(const Device d, cudaStream_t st, const CflParams& cp)
+{
+    const int hu[3] = {VTXBUF_UUX, VTXBUF_UUY, VTXBUF_UUZ};
+    ReduceArgs a;
+    long long blocks;
+    if (reduce_args(d, RTYPE_MAX, RED_VEC, hu, a, blocks) != AC_SUCCESS)
+        return AC_FAILURE;
+    reduce3_kernel<256><<<(unsigned)blocks, 256, 0, st>>>(a);
+    ACB_CUDA_CHECK(cudaGetLastError());
+    cfl_kernel<<<1, 32, 0, st>>>(d->red_result, d->cfl, cp);
+    ACB_CUDA_CHECK(cudaGetLastError());
+    d->launches += 2;
+    const int3 m0 = make_int3(0, 0, 0);
+    const int3 m1 = make_int3(d->L.mx, d->L.my, d->L.mz);
+    const int3 n0 = make_int3(NGHOST, NGHOST, NGHOST);
+    const int3 n1 = make_int3(NGHOST + d->L.nx, NGHOST + d->L.ny, NGHOST + d->L.nz);
+    for (int s = 0; s < 3; ++s) {
+        if (launch_halo(d, st, m0, m1, 0, NUM_VTXBUF_HANDLES) != AC_SUCCESS)
+            return AC_FAILURE;
+        if (launch_solve(d, st, s, n0, n1, d->cfl) != AC_SUCCESS)
+            return AC_FAILURE;
+        d->cur ^= 1;
+    }
+    return AC_SUCCESS;
 }
 
 // ---------------------------------------------------------------------------
@@ -978,6 +1161,8 @@ acDeviceCreate(const int id, const AcMeshInfo config, Device* device_handle)
     ACB_CUDA_CHECK(cudaMallocHost((void**)&d->h_result, 3 * sizeof(double)));
     ACB_CUDA_CHECK(cudaMalloc((void**)&d->status, sizeof(unsigned)));
     ACB_CUDA_CHECK(cudaMemset(d->status, 0, sizeof(unsigned)));
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->cfl, 3 * sizeof(double)));
+    ACB_CUDA_CHECK(cudaMemset(d->cfl, 0, 3 * sizeof(double)));
     if (stage_create(&d->stage, (size_t)d->L.mx * d->L.my * d->L.mz) != AC_SUCCESS)
         return AC_FAILURE;
 
@@ -1015,6 +1200,7 @@ acDeviceDestroy(Device device)
     cudaFree(device->red_result);
     cudaFreeHost(device->h_result);
     cudaFree(device->status);
+    cudaFree(device->cfl);
     if (device->xfer)
         cudaFree(device->xfer);
     stage_destroy(&device->stage);
@@ -1646,43 +1832,66 @@ acDeviceIntegrateSteps(const Device device, const Stream stream, const AcReal dt
     const unsigned long long base = (device->uniform_version << 8) ^
                                     ((unsigned long long)device->solve_cfg << 2) ^
                                     ((unsigned long long)stream << 40) ^ 1ull;
-    for (int i = 0; i < num_steps; ++i) {
-        const int p = device->cur;
-        // a captured step contains the ghost fill only when the ghosts were stale
-        const unsigned long long key = base ^ (device->ghost_ok[p] ? 2ull : 0ull);
-        if (!device->graph[p] || device->graph_key[p] != key) {
-            if (device->graph[p])
-                cudaGraphExecDestroy(device->graph[p]);
-            device->graph[p] = nullptr;
-            cudaGraph_t g;
-            ACB_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            const unsigned long long before = device->launches;
-            const AcResult rc               = enqueue_step(device, st);
-            ACB_CUDA_CHECK(cudaStreamEndCapture(st, &g));
-            device->cur               = p; // capture advanced the roles; replay does it below
-            device->graph_launches[p] = device->launches - before;
-            device->graph_ghost[p][0] = device->ghost_ok[0];
-            device->graph_ghost[p][1] = device->ghost_ok[1];
-            device->graph_lo[p][0]    = device->lo_stale[0];
-            device->graph_lo[p][1]    = device->lo_stale[1];
-            device->launches          = before;
-            if (rc != AC_SUCCESS) {
-                cudaGraphDestroy(g);
-                return AC_FAILURE;
-            }
-            ACB_CUDA_CHECK(cudaGraphInstantiate(&device->graph[p], g, 0));
-            cudaGraphDestroy(g);
-            device->graph_key[p] = key;
-        }
-        ACB_CUDA_CHECK(cudaGraphLaunch(device->graph[p], st));
-        device->write_epoch++; // the replayed solves wrote both blocks
-        device->launches += device->graph_launches[p];
-        device->ghost_ok[0] = device->graph_ghost[p][0]; // as the captured step left them
-        device->ghost_ok[1] = device->graph_ghost[p][1];
-        device->lo_stale[0] = device->graph_lo[p][0];
-        device->lo_stale[1] = device->graph_lo[p][1];
-        device->cur ^= 1; // three swaps per step
-    }
+    return replay_steps(device, st, STEP_FIXED, base, 0.0, num_steps,
+                        [](const Device d, cudaStream_t s) { return enqueue_step(d, s); });
+}
+
+AcResult
+acDeviceIntegrateStepCFL(const Device device, const Stream stream, const AcReal timescale)
+{
+    cudaSetDevice(device->id);
+    CflParams cp;
+    if (cfl_params(device, timescale, cp) != AC_SUCCESS)
+        return AC_FAILURE;
+    return enqueue_step_cfl(device, stream_of(device, stream), cp);
+}
+
+AcResult
+acDeviceIntegrateStepsCFL(const Device device, const Stream stream, const AcReal timescale,
+                          const int num_steps)
+{
+    cudaSetDevice(device->id);
+    if (num_steps <= 0)
+        return AC_SUCCESS;
+    CflParams cp;
+    if (cfl_params(device, timescale, cp) != AC_SUCCESS)
+        return AC_FAILURE;
+    if (prepare_kernels_once() != AC_SUCCESS || ensure_maps(device) != AC_SUCCESS)
+        return AC_FAILURE;
+    const cudaStream_t st = stream_of(device, stream);
+    const unsigned long long base = (device->uniform_version << 8) ^
+                                    ((unsigned long long)device->solve_cfg << 2) ^
+                                    ((unsigned long long)stream << 40) ^ 1ull;
+    return replay_steps(device, st, STEP_CFL, base, (double)timescale, num_steps,
+                        [cp](const Device d, cudaStream_t s) { return enqueue_step_cfl(d, s, cp); });
+}
+
+AcResult
+acDeviceGetTimestepRecord(const Device device, const Stream stream, AcReal* dt, double* time,
+                          unsigned long long* steps)
+{
+    cudaSetDevice(device->id);
+    const cudaStream_t st = stream_of(device, stream);
+    double h[3];
+    ACB_CUDA_CHECK(cudaMemcpyAsync(h, device->cfl, sizeof(h), cudaMemcpyDeviceToHost, st));
+    ACB_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (dt)
+        *dt = (AcReal)h[0];
+    if (time)
+        *time = h[1];
+    if (steps)
+        *steps = (unsigned long long)h[2];
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceSetSimulationTime(const Device device, const Stream stream, const double time)
+{
+    cudaSetDevice(device->id);
+    const cudaStream_t st = stream_of(device, stream);
+    const double h[3]     = {0.0, time, 0.0};
+    ACB_CUDA_CHECK(cudaMemcpyAsync(device->cfl, h, sizeof(h), cudaMemcpyHostToDevice, st));
+    ACB_CUDA_CHECK(cudaStreamSynchronize(st));
     return AC_SUCCESS;
 }
 

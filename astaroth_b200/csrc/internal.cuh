@@ -39,6 +39,9 @@ struct SolveConfig {
     // substeps 0, 1, 2, and 2 with helical forcing (single mesh only): a
     // SolveKernelFn, or an EnsKernelFn in the ensemble table
     const void* kern[4];
+    // single mesh: substeps 0, 1, 2 reading the time step from device memory
+    // (null in the ensemble table)
+    const void* kern_dt[3];
 };
 
 // "tile32x8_ring9", "..._tmacentre" when the centre values are staged by TMA
@@ -69,10 +72,16 @@ make_solve_config()
     c.kern[0] = (const void*)solve_kernel<Cfg, 0, ENS>;
     c.kern[1] = (const void*)solve_kernel<Cfg, 1, ENS>;
     c.kern[2] = (const void*)solve_kernel<Cfg, 2, ENS>;
-    if constexpr (ENS)
-        c.kern[3] = nullptr;
-    else
-        c.kern[3] = (const void*)solve_kernel<Cfg, 3, ENS>;
+    if constexpr (ENS) {
+        c.kern[3]    = nullptr;
+        c.kern_dt[0] = c.kern_dt[1] = c.kern_dt[2] = nullptr;
+    }
+    else {
+        c.kern[3]    = (const void*)solve_kernel<Cfg, 3, ENS>;
+        c.kern_dt[0] = (const void*)solve_kernel<Cfg, 0, ENS, true>;
+        c.kern_dt[1] = (const void*)solve_kernel<Cfg, 1, ENS, true>;
+        c.kern_dt[2] = (const void*)solve_kernel<Cfg, 2, ENS, true>;
+    }
     return c;
 }
 

@@ -61,6 +61,10 @@ struct SolveParams {
     // helical forcing, applied after the update at s = 2 when `forcing` != 0
     int forcing;
     T fk[3], ff_re[3], ff_im[3], fcphi, fsphi, fscale, fxs[3], fds[3];
+    // time step chosen on the device (acDeviceIntegrateStepCFL): the kernels
+    // built with DTDEV take rkB = (T)(rk_beta * *dt_dev) instead of rkB above
+    const double* dt_dev;
+    double rk_beta;
 };
 
 struct SolveGeom {
@@ -891,7 +895,7 @@ member_of(const MemberDesc<T>* md, int n, long long t)
 // One task of a consumer warp: the planes of one (tile, z segment) column.
 // Waits for the ring, computes and stores every output plane, releases the
 // slots, and advances the plane counter q. Returns false if the CTA aborts.
-template <class Cfg, int STEP, bool ENS, class PT>
+template <class Cfg, int STEP, bool ENS, bool DTDEV, class PT>
 __device__ __forceinline__ bool
 consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
              long long lt, state_t* out, float* in_lo, float* out_lo, const void* ring,
@@ -913,7 +917,10 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
     const int i     = tg.i0 + tx;
     const int j     = tg.j0 + ty;
     const bool act  = (i >= gv.start.x) && (i < gv.end.x) && (j < gv.end.y);
-    const T rkA     = a.P.rkA, rkB = a.P.rkB;
+    const T rkA     = a.P.rkA;
+    T rkB           = a.P.rkB;
+    if constexpr (DTDEV)
+        rkB = (T)(a.P.rk_beta * *a.P.dt_dev);
     // this thread's column in a ring slot (elements)
     const int col = (ty + NGHOST) * BX + (tx + 4);
 
@@ -1117,7 +1124,9 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
 template <bool ENS>
 using SolveKernelArgs = typename std::conditional<ENS, EnsSolveArgs<AcReal>, SolveArgs<AcReal>>::type;
 
-template <class Cfg, int STEP, bool ENS>
+// DTDEV: the time step is read from device memory (SolveParams::dt_dev), for
+// steps whose time step the device chooses; single meshes, no forcing.
+template <class Cfg, int STEP, bool ENS, bool DTDEV = false>
 __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     solve_kernel(const __grid_constant__ CUtensorMap tin,
                  const __grid_constant__ SolveKernelArgs<ENS> a,
@@ -1266,12 +1275,12 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
             const int m             = member_of(a.members, a.nmembers, tg_);
             const MemberDesc<T>* md = a.members + m;
             const SolveGeom gv      = md->g;
-            ok = consume_task<Cfg, STEP, ENS>(a, gv, a.mp[m], tg_ - md->task_begin, md->out,
+            ok = consume_task<Cfg, STEP, ENS, DTDEV>(a, gv, a.mp[m], tg_ - md->task_begin, md->out,
                                               md->in_lo, md->out_lo, ring, full, empty,
                                               &abort_flag, q, centre, full_c, empty_c, oq);
         }
         else {
-            ok = consume_task<Cfg, STEP, ENS>(a, a.g, a.P, t, a.out, a.in_lo, a.out_lo, ring, full,
+            ok = consume_task<Cfg, STEP, ENS, DTDEV>(a, a.g, a.P, t, a.out, a.in_lo, a.out_lo, ring, full,
                                               empty, &abort_flag, q, centre, full_c, empty_c,
                                               oq);
         }

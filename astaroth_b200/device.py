@@ -124,6 +124,26 @@ class Device:
         _check(self.lib.acDeviceIntegrateSteps(self.handle, stream, dt, n),
                "acDeviceIntegrateSteps")
 
+    # --- steps whose time step is chosen on the device ----------------------
+    def integrate_step_cfl(self, timescale: float = 1.0, stream: int = 0) -> None:
+        _check(self.lib.acDeviceIntegrateStepCFL(self.handle, stream, timescale),
+               "acDeviceIntegrateStepCFL")
+
+    def integrate_steps_cfl(self, n: int, timescale: float = 1.0, stream: int = 0) -> None:
+        _check(self.lib.acDeviceIntegrateStepsCFL(self.handle, stream, timescale, n),
+               "acDeviceIntegrateStepsCFL")
+
+    def timestep_record(self, stream: int = 0) -> tuple[float, float, int]:
+        """(dt of the last such step, simulated time, steps taken)."""
+        dt, t, k = self.prec.real(), C.c_double(), C.c_ulonglong()
+        _check(self.lib.acDeviceGetTimestepRecord(self.handle, stream, C.byref(dt), C.byref(t),
+                                                  C.byref(k)), "acDeviceGetTimestepRecord")
+        return float(dt.value), float(t.value), int(k.value)
+
+    def set_simulation_time(self, t: float, stream: int = 0) -> None:
+        _check(self.lib.acDeviceSetSimulationTime(self.handle, stream, t),
+               "acDeviceSetSimulationTime")
+
     def set_forcing(self, enabled: bool) -> None:
         _check(self.lib.acDeviceSetForcing(self.handle, int(bool(enabled))), "acDeviceSetForcing")
 

@@ -54,6 +54,8 @@ ASTAROTH_B200_H = [
     "acDeviceGetCudaStream", "acDeviceGetLaunchCount",
     "acDeviceSetSolveConfig", "acDeviceGetSolveConfig", "acSolveConfigName",
     "acDeviceGetMemoryFootprint", "acDeviceIntegrateStep", "acDeviceIntegrateSteps",
+    "acDeviceIntegrateStepCFL", "acDeviceIntegrateStepsCFL", "acDeviceGetTimestepRecord",
+    "acDeviceSetSimulationTime",
     "acDeviceSetForcing", "acDeviceLoadVertexBufferDouble", "acDeviceStoreVertexBufferDouble",
     "acDeviceReduceScalDouble", "acDeviceReduceVecDouble", "acReduceScalNoAlloc",
     "acForcingParamsFromUniforms", "acForcingParamsGenerate", "acDeviceLoadForcingParams",
@@ -161,6 +163,11 @@ def _declare(lib: C.CDLL, prec: abi.Precision) -> None:
         "acDeviceGetMemoryFootprint": (res, [Dev, C.POINTER(C.c_size_t)]),
         "acDeviceIntegrateStep": (res, [Dev, i, R]),
         "acDeviceIntegrateSteps": (res, [Dev, i, R, i]),
+        "acDeviceIntegrateStepCFL": (res, [Dev, i, R]),
+        "acDeviceIntegrateStepsCFL": (res, [Dev, i, R, i]),
+        "acDeviceGetTimestepRecord": (res, [Dev, i, C.POINTER(R), C.POINTER(C.c_double),
+                                            C.POINTER(C.c_ulonglong)]),
+        "acDeviceSetSimulationTime": (res, [Dev, i, C.c_double]),
         "acDeviceSetForcing": (res, [Dev, i]),
         "acDeviceLoadVertexBufferDouble": (res, [Dev, i, i, C.c_void_p]),
         "acDeviceStoreVertexBufferDouble": (res, [Dev, i, i, C.c_void_p]),

@@ -17,8 +17,11 @@ acDeviceIntegrateSubstep, acDeviceSwapBuffers). Inputs are larger than L2
 Beside the headline line: the FP64 and FP32 libraries on the same steps (and
 the per-field error against FP64), an end-to-end run from pinned host memory,
 the 64-member ensemble, the 256^3 FP32 and FP64 runs with four reductions read
-back every step, and the forced large-mesh run (1024^3 mixed, helical forcing
-from a seeded generator and four FP64 diagnostics every step).
+back every step, simulation loops whose time step follows the state (64^3 and
+128^3 FP32: the time step chosen on the host after a synchronising reduction,
+as the reference standalone does, against the time step chosen on the device),
+and the forced large-mesh run (1024^3 mixed, helical forcing from a seeded
+generator and four FP64 diagnostics every step).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -59,6 +62,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-member ensemble")
+    ap.add_argument("--no-cfl", action="store_true",
+                    help="skip the loops whose time step follows the state")
     ap.add_argument("--no-forced", action="store_true",
                     help="skip the forced large-mesh run (helical forcing + diagnostics)")
     ap.add_argument("--forced-n", type=int, default=1024, help="mesh size of the forced run")
@@ -586,6 +591,65 @@ def diagnostics_run(n: int, steps: int, warmup: int, ranks, gpu: int) -> dict:
     return out
 
 
+def cfl_run(sizes, steps: int, warmup: int, ranks, gpu: int) -> dict:
+    """Simulation loops whose time step follows the state (FP32, seeded state
+    of the headline workload at smaller n, AC_cdt = 0.4, AC_cdtv = 0.3): the
+    reference standalone's loop, each step a synchronising max |u| reduction
+    read back, the Courant time step on the host (host_timestep) and an RK3
+    step, against acDeviceIntegrateStepsCFL, where the reduction, the time
+    step and the RK3 step run on the device from one CUDA graph per step.
+    Steps per second of each, timed by CUDA events on the Device's stream."""
+    import torch
+
+    from astaroth_b200 import Device, abi
+
+    def host_timestep(info, umax):
+        g = lambda k: abi.get_real(info, k)  # noqa: E731
+        dsmin = min(g("dsx"), g("dsy"), g("dsz"))
+        uu_dt = g("cdt") * dsmin / (abs(umax) + math.sqrt(g("cs2_sound")))
+        visc_dt = g("cdtv") * dsmin * dsmin / max(g("nu_visc"), g("eta"), g("gamma"), 0.0)
+        return min(uu_dt, visc_dt)
+
+    out = {"precision": "FP32", "steps": steps,
+           "host_loop": "acDeviceReduceVec(MAX |u|) read back + host_timestep + acDeviceIntegrateStep",
+           "device_loop": "acDeviceIntegrateStepsCFL (reduction, time step, RK3 step in one graph)"}
+    for n in sizes:
+        host = host_mesh("sp", n)
+        abi.set_real(host.info, "cs2_sound", 1.0)
+        dev = Device("sp", host.info, gpu)
+        try:
+            dev.load_mesh(host)
+            st = torch.cuda.ExternalStream(dev.cuda_stream(0))
+
+            def host_step():
+                u = dev.reduce_vec(abi.RTYPE_MAX, abi.VTXBUF_UUX, abi.VTXBUF_UUY, abi.VTXBUF_UUZ)
+                dev.integrate_step(host_timestep(host.info, u))
+
+            def timed(fn, k):
+                for _ in range(warmup):
+                    fn()
+                dev.synchronize()
+                ranks.barrier()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                for _ in range(k):
+                    fn()
+                e1.record(st)
+                e1.synchronize()
+                return ranks.max(e0.elapsed_time(e1)) / k
+
+            host_ms = timed(host_step, steps)
+            dev_ms = timed(lambda: dev.integrate_steps_cfl(1), steps)
+            dt, t, k = dev.timestep_record()
+            out[f"{n}^3"] = {"host_loop_ms_per_step": host_ms, "device_loop_ms_per_step": dev_ms,
+                             "speedup": host_ms / dev_ms, "last_dt": dt, "device_steps": k}
+        finally:
+            dev.destroy()
+            del host
+            torch.cuda.empty_cache()
+    return out
+
+
 def profile_traffic(name: str):
     """Per-launch DRAM bytes of the dominant kernel from a committed ncu
     summary (a line `traffic_bytes_per_launch: <value>`), else None."""
@@ -711,6 +775,10 @@ def run_ours(args) -> None:
     if not args.no_diagnostics:
         diagnostics = diagnostics_run(256, 100, max(args.warmup, 3), ranks, gpu)
 
+    cfl = None
+    if not args.no_cfl:
+        cfl = cfl_run((64, 128), 200, max(args.warmup, 3), ranks, gpu)
+
     forced = None
     if not args.no_forced:
         torch.cuda.empty_cache()
@@ -737,7 +805,8 @@ def run_ours(args) -> None:
                              "solve_ms_per_substep": res["solve_ms_per_substep"]},
                 "clocks": res["clocks"], "gpu_launches": res["launches"],
                 "e2e": e2e, "cpu_baseline": cpu, "variants": variants, "errors": errors,
-                "ensemble": ensemble, "diagnostics_256": diagnostics, "forced": forced}
+                "ensemble": ensemble, "diagnostics_256": diagnostics, "cfl_loop": cfl,
+                "forced": forced}
         print(json.dumps(line), flush=True)
     ranks.close()
 

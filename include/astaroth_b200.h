@@ -62,6 +62,42 @@ AcResult acDeviceIntegrateStep(const Device device, const Stream stream, const A
 AcResult acDeviceIntegrateSteps(const Device device, const Stream stream, const AcReal dt,
                                 const int num_steps);
 
+/* ---- steps whose time step is chosen on the device --------------------- */
+
+/* One full RK3 step whose dt is the reference standalone's Courant time step
+ * (samples/standalone/simulation.cc:429-436, model/host_timestep.cc:33-60,
+ * with the shipped module's LSINK = LBFIELD = 0), evaluated on the device from
+ * the current state:
+ *   dt = timescale * min(AC_cdt dsmin / (max|u| + sqrt(AC_cs2_sound)),
+ *                        AC_cdtv dsmin^2 / max(AC_nu_visc, AC_eta, AC_gamma))
+ * with max|u| over the interior (the reduction acDeviceReduceVec(RTYPE_MAX) of
+ * uux, uuy, uuz, rounded to AcReal) and dsmin = AC_dsmin, or the smallest of
+ * AC_dsx, AC_dsy, AC_dsz where AC_dsmin is unset. The standalone does this on
+ * the host with a synchronising reduction each step; here the reduction, the
+ * time step and the three substeps are queued on `stream` and nothing returns
+ * to the host. The dt used, the accumulated simulated time and the number of
+ * such steps are kept on the device (acDeviceGetTimestepRecord). Asynchronous.
+ * AC_FAILURE if AC_cdt, AC_cdtv, the spacings or timescale are not positive, or
+ * if forcing is enabled (its amplitude depends on dt on the host). The
+ * reduction uses the Device's reduction scratch: do not run reductions of the
+ * same Device on another stream at the same time. */
+AcResult acDeviceIntegrateStepCFL(const Device device, const Stream stream, const AcReal timescale);
+
+/* `num_steps` such steps replayed from one captured CUDA graph (built on first
+ * use, rebuilt when the uniforms, the configuration or timescale change). */
+AcResult acDeviceIntegrateStepsCFL(const Device device, const Stream stream,
+                                   const AcReal timescale, const int num_steps);
+
+/* The time-step record of those steps: dt of the last one, the simulated time
+ * (the sum of their dt, from the value acDeviceSetSimulationTime set) and how
+ * many were taken. Synchronises `stream`; null pointers are skipped. */
+AcResult acDeviceGetTimestepRecord(const Device device, const Stream stream, AcReal* dt,
+                                   double* time, unsigned long long* steps);
+
+/* Sets the record's simulated time (and clears its dt and step count).
+ * Synchronises `stream`. */
+AcResult acDeviceSetSimulationTime(const Device device, const Stream stream, const double time);
+
 /* Enables the helical forcing term at the last substep
  * (acc/mhd_solver/stencil_kernel.ac:611-648,713-717; off in the reference's
  * shipped module). Its parameters are the AC_forcing_* / AC_k_force* /
