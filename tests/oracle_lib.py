@@ -10,6 +10,7 @@ this module. It wraps
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -140,3 +141,20 @@ def normwise_error(candidate: np.ndarray, model: np.ndarray) -> float:
     den = np.max(np.abs(m))
     num = np.max(np.abs(c - m))
     return float(num / den) if den > 0 else float(num)
+
+
+def cfl_dt(prec, info, umax: float, timescale: float = 1.0) -> float:
+    """The Courant time step as the library evaluates it on the device
+    (astaroth_b200/csrc/device.cu: cfl_kernel): the reference standalone's
+    host_timestep (samples/standalone/model/host_timestep.cc:33-60, vAmax = 0)
+    in double precision instead of long double, umax rounded to AcReal first,
+    AC_dsmin or else the smallest spacing, the product with timescale in AcReal."""
+    R = prec.np_dtype
+    g = lambda k: abi.get_real(info, k)  # noqa: E731
+    u = float(R(umax))
+    dsmin = g("dsmin")
+    if not dsmin > 0:
+        dsmin = min(g("dsx"), g("dsy"), g("dsz"))
+    uu_dt = g("cdt") * dsmin / (abs(u) + math.sqrt(g("cs2_sound")))
+    visc_dt = g("cdtv") * dsmin * dsmin / max(max(g("nu_visc"), g("eta")), max(g("gamma"), 0.0))
+    return float(R(timescale) * R(min(uu_dt, visc_dt)))
