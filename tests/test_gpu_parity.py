@@ -20,7 +20,7 @@ import oracle_lib as O
 
 pytestmark = pytest.mark.gpu
 FLAVOURS = ("sp", "dp", "mixed")
-TOL = {"sp": 1e-5, "dp": 1e-12, "mixed": 1e-5}
+TOL = {"sp": 1e-5, "dp": 1e-12, "mixed": 1e-6}
 PHYS = dict(gamma=5.0 / 3.0, nu_visc=5e-3, eta=5e-3, cs_sound=1.0, cp_sound=1.0)
 
 
@@ -154,6 +154,7 @@ def test_ragged_mesh_vs_oracle(flavour):
     om = O.OracleMesh("f80", fields, nx, ny, nz)
     om.step(O.params_from(info), dt, steps)
     errs = [O.normwise_error(interior(out[w]), om.interior(w)) for w in range(8)]
+    print(flavour, ["%.2e" % e for e in errs])
     assert max(errs) <= TOL[flavour], errs
 
 
@@ -315,6 +316,7 @@ def test_forcing_vs_oracle(flavour):
     om = O.OracleMesh("f80", fields, n, n, n)
     om.step(p, dt, steps)
     errs = [O.normwise_error(interior(out[w]), om.interior(w)) for w in range(8)]
+    print("forcing", flavour, ["%.2e" % e for e in errs])
     assert max(errs) <= TOL[flavour], errs
 
 
@@ -350,6 +352,7 @@ def test_generated_forcing_each_step_vs_oracle(flavour):
                           ff_re=list(fp.ff_hel_re), ff_im=list(fp.ff_hel_im))
         om.step(p, dt, 1)
     errs = [O.normwise_error(interior(out[w]), om.interior(w)) for w in range(8)]
+    print("generated forcing", flavour, ["%.2e" % e for e in errs])
     assert max(errs) <= TOL[flavour], errs
     # the forcing moved the velocity well beyond the tolerance
     free = O.OracleMesh("f80", fields, n, n, n)
@@ -368,7 +371,7 @@ def test_mixed_tracks_fp64():
     es = [O.normwise_error(interior(s[w]), interior(d[w])) for w in range(8)]
     print("mixed vs dp", ["%.2e" % e for e in em])
     print("sp    vs dp", ["%.2e" % e for e in es])
-    assert max(em) <= 1e-5
+    assert max(em) <= 1e-6
 
 
 @pytest.mark.parametrize("flavour", ["sp", "mixed"])
