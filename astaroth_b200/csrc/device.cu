@@ -373,8 +373,9 @@ acb_host::make_params(const AcMeshInfo& uniforms, const Layout& L, int step, int
                            gn.z > 0 ? gn.z : L.nz};
         const double ds[3] = {rp[AC_dsx], rp[AC_dsy], rp[AC_dsz]};
         for (int c = 0; c < 3; ++c) {
-            P.fds[c] = (AcReal)ds[c];
-            P.fxs[c] = (AcReal)(2.0 * M_PI / (ds[c] * nn[c]));
+            P.fds[c]   = (AcReal)ds[c];
+            P.fxs[c]   = (AcReal)(2.0 * M_PI / (ds[c] * nn[c]));
+            P.fxs_d[c] = 2.0 * M_PI / (ds[c] * nn[c]);
         }
     }
     return P;
