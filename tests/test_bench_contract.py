@@ -51,3 +51,14 @@ def test_traffic_and_peak_come_from_committed_files():
     assert t is not None and abs(t / (192 * 512 ** 3) - 1.0) < 0.10
     peak, kind = bench.measured_peak_hbm()
     assert kind == "measured" and 5000.0 < peak < 8000.0
+
+
+def test_cpu_oracle_sample_reports_all_cores():
+    """The multi-core CPU figure: the oracle's FP64 solver with OpenMP on every
+    host core, a bounded sample."""
+    import bench
+
+    r = bench.cpu_oracle_sample(budget_s=0.2, n=16)
+    assert r["kind"] == "port" and r["unit"] == bench.UNIT
+    assert r["cores"] == (os.cpu_count() or 1)
+    assert r["value"] > 0 and "FP64" in r["sample"]
