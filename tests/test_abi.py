@@ -180,3 +180,34 @@ def test_reference_ctest_links_unchanged():
                     f"-L{library.LIBDIR}", "-lastaroth_sp", f"-Wl,-rpath,{library.LIBDIR}"],
                    check=True)
     assert os.path.exists(ctest_binary())
+
+
+def _header_arity():
+    """Parameter count of every function include/*.h declares."""
+    arity = {}
+    for h in ("astaroth.h", "astaroth_utils.h", "astaroth_b200.h"):
+        text = open(os.path.join(REPO, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        text = re.sub(r"static inline[^{]*\{.*?\n\}", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?(?:AcResult|AcReal|int|Node|Error|bool|const char\s*\*)"
+                             r"\s+(ac\w+)\s*\(([^;{]*?)\)\s*;", text, flags=re.M | re.S):
+            params = " ".join(m.group(2).split())
+            arity[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return arity
+
+
+@pytest.mark.parametrize("flavour", FLAVOURS)
+def test_binding_prototypes_match_header_arity(flavour):
+    """Every prototype the Python binding declares takes as many arguments as
+    the header declares (catches a binding left behind by a header change)."""
+    arity = _header_arity()
+    lib = library.load(flavour)
+    checked = 0
+    for name in library.ALL_SYMBOLS:
+        fn = getattr(lib, name, None)
+        if fn is None or fn.argtypes is None or name not in arity:
+            continue
+        assert len(fn.argtypes) == arity[name], (name, len(fn.argtypes), arity[name])
+        checked += 1
+    assert checked >= 60, checked
