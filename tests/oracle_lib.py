@@ -20,6 +20,9 @@ from astaroth_b200 import abi
 
 REPO = abi.REPO
 ORACLE_DIR = os.path.join(REPO, "oracle")
+# the reference sources (present only where the checker is built; the built
+# files travel with the repository)
+REFERENCE = os.environ.get("ASTAROTH_REFERENCE", "/root/reference")
 KIND_DTYPE = {"f32": np.float32, "f64": np.float64, "f80": np.longdouble}
 
 

@@ -169,7 +169,7 @@ def ctest_binary():
 
 
 def test_reference_ctest_links_unchanged():
-    src = "/root/reference/samples/ctest/main.c"
+    src = os.path.join(O.REFERENCE, "samples", "ctest", "main.c")
     if not os.path.exists(src):
         if os.path.exists(ctest_binary()):
             return

@@ -1,8 +1,10 @@
 """Parity of the CUDA path (through the C ABI) with the CPU oracle.
 
 Tolerances (normwise per field: max|cand - model| / max|model| over the interior):
-  FP32  <= 1e-5     FP64 <= 1e-12     (vs the long-double oracle)
-  mixed <= 1e-5 vs the oracle; its distance to the FP64 GPU result is reported
+  FP32  <= 1e-5     FP64 <= 1e-12     mixed <= 1e-6
+against the long-double oracle (the f64 oracle at 256^3 and above, where the
+long-double build would take minutes); mixed also <= 1e-6 against the FP64 GPU
+path.
 Load/store, ghost fill, sub-box updates, graph replay and tile choice are
 checked bit-exactly. Full-size behaviour is checked through size-independent
 properties (periodic-shift equivariance, reductions of a stored mesh).
