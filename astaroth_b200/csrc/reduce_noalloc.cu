@@ -26,7 +26,11 @@
 // host the name is only a stand-in). On its first call on a device, the entry
 // point asks the runtime for the device address of each array with
 // cudaGetSymbolAddress, with that device current, and caches it per device.
-// That first call should therefore come before any stream capture.
+// That first call should therefore come before any stream capture. The cache
+// lives as long as the process: after cudaDeviceReset (or the destruction of
+// the device's primary context) the library's module is loaded anew at other
+// addresses, and the cached ones would point into freed memory, so resetting a
+// device between calls is not supported.
 #include <math.h>
 #include <stdio.h>
 

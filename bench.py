@@ -67,6 +67,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-forced", action="store_true",
                     help="skip the forced large-mesh run (helical forcing + diagnostics)")
     ap.add_argument("--forced-n", type=int, default=1024, help="mesh size of the forced run")
+    ap.add_argument("--no-oracle", action="store_true",
+                    help="skip the comparisons with the f64 oracle (512^3 after 2 steps; "
+                         "256^3 diagnostics over 100 steps)")
     ap.add_argument("--no-diagnostics", action="store_true",
                     help="skip the 256^3 FP32/FP64 run with reductions every step")
     return ap.parse_args(argv)
@@ -193,10 +196,12 @@ def workload_info(prec, n: int):
     return abi.make_info(prec, n, n, n, dsx=ds, dsy=ds, dsz=ds, **PHYS)
 
 
-def host_mesh(flavour: str, n: int, pinned: bool = True):
-    """The seeded initial state as a pinned host AcMesh of the flavour's AcReal.
-    Values are generated on the GPU (bit-identical to the numpy generator),
-    rounded to float32 once; the FP64 library gets the same float32 values."""
+def host_mesh(flavour: str, n: int, pinned: bool = True, velocity_mode: float = 0.1):
+    """The seeded initial state as a pinned host AcMesh of the flavour's AcReal:
+    1e-3 noise (seed 1) plus the k = 2 velocity mode of amplitude
+    velocity_mode. Values are generated on the GPU (bit-identical to the numpy
+    generator), rounded to float32 once; the FP64 library gets the same
+    float32 values."""
     import torch
 
     from astaroth_b200 import abi, init
@@ -206,7 +211,7 @@ def host_mesh(flavour: str, n: int, pinned: bool = True):
     tdt = torch.float64 if prec.double else torch.float32
     host = abi.HostMesh(prec, info, pinned=pinned)
     gen = init.workload_fields_torch(n, n, n, torch.float32, seed=1, amplitude=1e-3,
-                                     velocity_mode=0.1, device="cuda")
+                                     velocity_mode=velocity_mode, device="cuda")
     for w, g in enumerate(gen):
         host.fields[w][...] = g.to(tdt).cpu().numpy()
     del gen
@@ -316,10 +321,10 @@ def e2e_run(flavour: str, host, steps: int, ranks) -> dict:
 
 
 def cpu_oracle_sample(budget_s: float = 6.0, n: int = 64) -> dict:
-    """The CPU restatement of the reference host solver (oracle/mhd_oracle.c)
-    in double precision with OpenMP on all host cores, on an n^3 sample of the
-    same physics: the multi-core CPU figure beside the reference's own
-    single-threaded solver."""
+    """The CPU restatement of the reference host solver (oracle/mhd_oracle.c,
+    its row-wise form) in double precision with OpenMP on the host cores this
+    process may use, on an n^3 sample of the same physics: the multi-core CPU
+    figure beside the reference's own single-threaded solver."""
     sys.path.insert(0, os.path.join(HERE, "tests"))
     import numpy as np
 
@@ -336,17 +341,26 @@ def cpu_oracle_sample(budget_s: float = 6.0, n: int = 64) -> dict:
         om.step(p, DT)
         steps += 1
     t = time.perf_counter() - t0
-    return {"value": n ** 3 * steps / t, "unit": UNIT, "cores": os.cpu_count() or 1,
-            "kind": "port",
-            "sample": f"{steps} RK3 steps of a {n}^3 mesh; oracle/mhd_oracle.c in FP64, "
-                      "OpenMP on all host cores"}
+    threads = O.omp_threads()
+    return {"value": n ** 3 * steps / t, "unit": UNIT, "cores": threads,
+            "cpus_available": len(os.sched_getaffinity(0)), "kind": "port",
+            "sample": f"{steps} RK3 steps of a {n}^3 mesh; oracle/mhd_oracle.c (row-wise form) "
+                      f"in FP64, OpenMP with {threads} threads"}
+
+
+# the reference's host utils as timed: its Release flags (-O3 on x86-64; the
+# pinning build, which also turns contraction off) and an AVX2/FMA build
+REF_BUILDS = {"": "-O3 -march=x86-64-v2 -ffp-contract=off",
+              "avx2": "-O3 -march=x86-64-v3 (AVX2, FMA contraction on)"}
 
 
 def cpu_reference_sample(budget_s: float = 12.0, n: int = 64, max_steps: int | None = None,
-                         warmup: int = 0) -> dict:
+                         warmup: int = 0, build: str | None = None) -> dict:
     """The reference's own host solver (src/utils/modelsolver.c acHostIntegrateStep,
-    built from its sources into oracle/_ref) on an n^3 sample of the same
-    physics; the oracle port (OpenMP) where that build is absent."""
+    FP32, built from its sources into oracle/_ref; its OpenMP pragmas are
+    commented out, so one thread) on an n^3 sample of the same physics; the
+    oracle port (OpenMP) where that build is absent. build None: the faster
+    of the two builds (one warm-up step of each decides)."""
     sys.path.insert(0, os.path.join(HERE, "tests"))
     import numpy as np
 
@@ -355,15 +369,25 @@ def cpu_reference_sample(budget_s: float = 12.0, n: int = 64, max_steps: int | N
 
     info = workload_info(abi.SP, n)
     fields = init.workload_fields(n, n, n, np.float32, seed=1, amplitude=1e-3, velocity_mode=0.1)
-    ref = O.ref_lib("sp")
-    if ref is not None:
+    libs = {b: O.ref_lib("sp", b) for b in REF_BUILDS}
+    libs = {b: l for b, l in libs.items() if l is not None}
+    if libs:
         hm = abi.HostMesh(abi.SP, info, fields)
+        if build is None:
+            pick = {}
+            for b, lib in libs.items():
+                t0 = time.perf_counter()
+                lib.acHostIntegrateStep(hm.cmesh, abi.SP.real(DT))
+                pick[b] = time.perf_counter() - t0
+            build = min(pick, key=pick.get)
+        ref = libs[build]
 
         def step():
             ref.acHostIntegrateStep(hm.cmesh, abi.SP.real(DT))
 
         kind, cores = "reference", 1
-        what = "reference src/utils/modelsolver.c acHostIntegrateStep (FP32), 1 thread"
+        what = ("reference src/utils/modelsolver.c acHostIntegrateStep (FP32), 1 thread, "
+                f"built {REF_BUILDS[build]}")
     else:
         om = O.OracleMesh("f32", fields, n, n, n)
         p = O.params_from(info)
@@ -371,8 +395,8 @@ def cpu_reference_sample(budget_s: float = 12.0, n: int = 64, max_steps: int | N
         def step():
             om.step(p, float(np.float32(DT)))
 
-        kind, cores = "port", os.cpu_count() or 1
-        what = "oracle/mhd_oracle.c (FP32 restatement), OpenMP on all cores"
+        kind, cores, build = "port", O.omp_threads(), "port"
+        what = f"oracle/mhd_oracle.c (FP32 restatement), OpenMP with {cores} threads"
     for _ in range(warmup):
         step()
     times = []
@@ -388,7 +412,52 @@ def cpu_reference_sample(budget_s: float = 12.0, n: int = 64, max_steps: int | N
     tot = sum(times)
     return {"value": n ** 3 * len(times) / tot, "unit": UNIT, "cores": cores, "kind": kind,
             "sample": f"{len(times)} RK3 steps of a {n}^3 mesh of the same physics; {what}",
-            "ms_per_step": 1e3 * tot / len(times), "steps": len(times)}
+            "ms_per_step": 1e3 * tot / len(times), "steps": len(times), "build": build,
+            "mesh": [n, n, n]}
+
+
+def oracle_errors(n: int, steps: int, gpu: int) -> dict:
+    """Per-field error of the three libraries against the f64 oracle at n^3:
+    the headline's seeded initial state, `steps` RK3 steps through
+    acDeviceIntegrateStep in each library, the oracle (row-wise form, OpenMP)
+    stepped from the same float32 values; max|x - x_oracle| / max|x_oracle| per
+    field over the interior, evaluated on the GPU in double precision."""
+    import torch
+
+    sys.path.insert(0, os.path.join(HERE, "tests"))
+    import oracle_lib as O
+    from astaroth_b200 import Device, abi
+
+    t0 = time.perf_counter()
+    host = host_mesh("sp", n)
+    om = O.OracleMesh("f64", host.fields, n, n, n)
+    om.step(O.params_from(workload_info(abi.DP, n)), DT, steps)
+    oracle_s = time.perf_counter() - t0
+    g = abi.NGHOST
+    out = {"metric": f"max|x - x_oracle| / max|x_oracle| per field after {steps} steps at "
+                     f"{n}^3 (f64 oracle, row-wise form)",
+           "fields": list(abi.VTXBUFS), "oracle_seconds": oracle_s,
+           "oracle_threads": O.omp_threads()}
+    for flav in ("mixed", "sp", "dp"):
+        h = host if flav != "dp" else host_mesh("dp", n)
+        dev = Device(flav, h.info, gpu)
+        try:
+            dev.load_mesh(h)
+            for _ in range(steps):
+                dev.integrate_step(DT)
+            dev.synchronize()
+            errs = []
+            for w in range(8):
+                a = torch.from_numpy(dev.store_double(w)).cuda()[g:-g, g:-g, g:-g]
+                b = torch.from_numpy(om.interior(w)).cuda()
+                errs.append(float((a - b).abs().max()) / float(b.abs().max()))
+                del a, b
+            out[{"mixed": "mixed_vs_oracle", "sp": "fp32_vs_oracle", "dp": "fp64_vs_oracle"}[flav]] = errs
+        finally:
+            dev.destroy()
+            torch.cuda.empty_cache()
+    del om, host
+    return out
 
 
 def ensemble_run(steps: int, ranks) -> dict:
@@ -567,19 +636,25 @@ def forced_run(n: int, steps: int, warmup: int, ranks, gpu: int) -> dict:
         torch.cuda.empty_cache()
 
 
-def diagnostics_run(n: int, steps: int, warmup: int, ranks, gpu: int) -> dict:
-    """The diagnostics workload: an n^3 mesh (256^3) of the seeded state in
+def diagnostics_run(n: int, steps: int, warmup: int, ranks, gpu: int,
+                    check_steps: int = 0) -> dict:
+    """The diagnostics workload: an n^3 mesh (256^3) of seeded 1e-3 noise in
     FP32 and in FP64, each step an RK3 step followed by max, min and rms of |u|
     and rms_exp of lnrho, each read back (FP64 accumulation); reported as
-    step-only time, step + diagnostics time and the time of one reduction."""
+    step-only time, step + diagnostics time and the time of one reduction.
+    With check_steps > 0, also the error of both libraries against the f64
+    oracle over that many steps from the initial state: every step's four
+    diagnostics (relative) and the final fields (normwise)."""
     import torch
 
     from astaroth_b200 import Device, abi
 
-    out = {"mesh": [n, n, n], "steps": steps, "warmup": warmup,
+    out = {"mesh": [n, n, n], "steps": steps, "warmup": warmup, "init": "seeded 1e-3 noise",
            "diagnostics": "max, min, rms of |u|; rms_exp of lnrho; each read back"}
+    if check_steps > 0:
+        out["errors_vs_oracle"] = diagnostics_errors(n, check_steps, gpu)
     for flav in ("sp", "dp"):
-        host = host_mesh(flav, n)
+        host = host_mesh(flav, n, velocity_mode=0.0)
         dev = Device(flav, host.info, gpu)
         try:
             dev.load_mesh(host)
@@ -614,6 +689,62 @@ def diagnostics_run(n: int, steps: int, warmup: int, ranks, gpu: int) -> dict:
         finally:
             dev.destroy()
             del host
+            torch.cuda.empty_cache()
+    return out
+
+
+def diagnostics_errors(n: int, steps: int, gpu: int) -> dict:
+    """FP32 and FP64 against the f64 oracle (row-wise form, OpenMP) over
+    `steps` RK3 steps of the diagnostics workload: after every step the four
+    diagnostics (relative error; the oracle's sums in long double) and at the
+    end every field (normwise, interior)."""
+    import torch
+
+    sys.path.insert(0, os.path.join(HERE, "tests"))
+    import oracle_lib as O
+    from astaroth_b200 import Device, abi
+
+    t0 = time.perf_counter()
+    host = host_mesh("sp", n, velocity_mode=0.0)
+    om = O.OracleMesh("f64", host.fields, n, n, n)
+    p = O.params_from(workload_info(abi.DP, n))
+    want = []
+    for _ in range(steps):
+        om.step(p, DT)
+        want.append(om.diagnostics())
+    out = {"steps": steps, "oracle": "f64, row-wise form", "oracle_seconds": time.perf_counter() - t0,
+           "oracle_threads": O.omp_threads(),
+           "metric": "per step: max over the four diagnostics of |x - x_oracle| / |x_oracle|; "
+                     "fields: max|x - x_oracle| / max|x_oracle| per field after the last step"}
+    U = (abi.VTXBUF_UUX, abi.VTXBUF_UUY, abi.VTXBUF_UUZ)
+    g = abi.NGHOST
+    cells = n ** 3
+    for flav in ("sp", "dp"):
+        h = host if flav == "sp" else host_mesh("dp", n, velocity_mode=0.0)
+        dev = Device(flav, h.info, gpu)
+        try:
+            dev.load_mesh(h)
+            per_step = []
+            for k in range(steps):
+                dev.integrate_step(DT)
+                got = (dev.reduce_vec_double(abi.RTYPE_MAX, *U),
+                       dev.reduce_vec_double(abi.RTYPE_MIN, *U),
+                       math.sqrt(dev.reduce_vec_double(abi.RTYPE_RMS, *U) / cells),
+                       math.sqrt(dev.reduce_scal_double(abi.RTYPE_RMS_EXP, abi.VTXBUF_LNRHO)
+                                 / cells))
+                per_step.append(max(abs(a - b) / abs(b) for a, b in zip(got, want[k])))
+            dev.synchronize()
+            fields = []
+            for w in range(8):
+                a = torch.from_numpy(dev.store_double(w)).cuda()[g:-g, g:-g, g:-g]
+                b = torch.from_numpy(om.interior(w)).cuda()
+                fields.append(float((a - b).abs().max()) / float(b.abs().max()))
+                del a, b
+            out[flav] = {"diagnostics_max_rel_error": max(per_step),
+                         "diagnostics_rel_error_last_step": per_step[-1],
+                         "fields": fields, "fields_max": max(fields)}
+        finally:
+            dev.destroy()
             torch.cuda.empty_cache()
     return out
 
@@ -713,15 +844,24 @@ def config_block(n: int, world: int) -> dict:
 
 
 def run_reference(args) -> None:
+    """The reference's own host solver on the box's cores: `steps` RK3 steps of
+    a 64^3 sample of the headline physics (the faster of its two builds), and
+    two steps of a 128^3 sample beside it. Rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return  # the reference CPU arm runs on rank 0 only
     r = cpu_reference_sample(n=64, max_steps=args.steps, warmup=args.warmup)
+    r128 = cpu_reference_sample(n=128, max_steps=2, warmup=0, build=r["build"])
+    cfg = config_block(64, 1)
+    cfg["workload"] = ("the headline workload's physics (seeded 1e-3 noise + k=2 velocity mode "
+                       "0.1, nu = eta = 5e-3, dt = 1e-3, dx = 2 pi / n) on a 64^3 sample; the "
+                       "reference's host solver in FP32")
+    cfg["samples"] = {"64^3": {k: r[k] for k in ("value", "ms_per_step", "steps")},
+                      "128^3": {k: r128[k] for k in ("value", "ms_per_step", "steps")}}
     line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": r["steps"], "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "impl": "reference",
-            "config": config_block(args.n, 1),
+            "data": "synthetic", "impl": "reference", "config": cfg,
             "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -783,6 +923,11 @@ def run_ours(args) -> None:
     dev.destroy()
     del host
     torch.cuda.empty_cache()
+    # the oracle runs on the host cores: one-GPU runs only
+    check = not args.no_oracle and ranks.world == 1
+    if check:
+        errors = errors or {}
+        errors["vs_oracle"] = oracle_errors(n, 2, gpu)
 
     e2e = None
     if not args.no_e2e:
@@ -800,7 +945,8 @@ def run_ours(args) -> None:
 
     diagnostics = None
     if not args.no_diagnostics:
-        diagnostics = diagnostics_run(256, 100, max(args.warmup, 3), ranks, gpu)
+        diagnostics = diagnostics_run(256, 100, max(args.warmup, 3), ranks, gpu,
+                                      check_steps=100 if check else 0)
 
     cfl = None
     if not args.no_cfl:

@@ -204,7 +204,9 @@ AcResult acDeviceReduceVecDouble(const Device device, const Stream stream,
  * Scratch lives in a fixed 128 KiB array of the library on each GPU, so
  * meshes with ny*nz > 1,048,576 are rejected (AC_FAILURE), calls that overlap
  * on the GPU race, and the first call on a device looks up the array's device
- * address (make that first call before any stream capture). */
+ * address (make that first call before any stream capture). The address is
+ * kept for the life of the process: a device reset (cudaDeviceReset) or a
+ * destroyed primary context between calls is not supported. */
 AcResult acReduceScalNoAlloc(void* cuda_stream, const ReductionType rtype, const AcReal* field,
                              const int nx, const int ny, const int nz, double* result);
 

@@ -54,15 +54,27 @@ def oracle_lib(kind: str) -> C.CDLL:
         lib.oracle_step.restype = C.c_int
         lib.oracle_step.argtypes = [C.c_void_p * 8, C.c_int, C.c_int, C.c_int,
                                     C.POINTER(OracleParams), C.c_double]
+        if kind != "f80":  # the row-wise form (float and double builds)
+            lib.oracle_step_rows.restype = C.c_int
+            lib.oracle_step_rows.argtypes = lib.oracle_step.argtypes
         lib.oracle_periodic.restype = None
         lib.oracle_periodic.argtypes = [C.c_void_p * 8, C.c_int, C.c_int, C.c_int]
         lib.oracle_reduce.restype = C.c_double
         lib.oracle_reduce.argtypes = [C.c_void_p * 8, C.c_int, C.c_int * 3, C.c_int, C.c_int,
                                       C.c_int, C.c_int, C.c_int]
+        lib.oracle_diagnostics.restype = None
+        lib.oracle_diagnostics.argtypes = [C.c_void_p * 8, C.c_int, C.c_int, C.c_int,
+                                           C.c_double * 4]
+        lib.oracle_omp_threads.restype = C.c_int
         lib.oracle_real_size.restype = C.c_int
         assert lib.oracle_real_size() == np.dtype(KIND_DTYPE[kind]).itemsize or kind == "f80"
         _LIBS[kind] = lib
     return _LIBS[kind]
+
+
+def omp_threads() -> int:
+    """Threads the oracle's OpenMP loops use in this process."""
+    return int(oracle_lib("f64").oracle_omp_threads())
 
 
 def params_from(info=None, **kw) -> OracleParams:
@@ -98,9 +110,14 @@ class OracleMesh:
         self.fields = [np.ascontiguousarray(f, dtype=KIND_DTYPE[kind]) for f in fields]
         self.n = (nx, ny, nz)
 
-    def step(self, params: OracleParams, dt: float, nsteps: int = 1) -> None:
+    def step(self, params: OracleParams, dt: float, nsteps: int = 1,
+             vertexwise: bool = False) -> None:
+        """nsteps RK3 steps. The float and double builds take the row-wise
+        evaluation (oracle_step_rows, bit-identical to the vertex-wise
+        oracle_step and many times faster) unless vertexwise is set."""
+        fn = self.lib.oracle_step if vertexwise or self.kind == "f80" else self.lib.oracle_step_rows
         for _ in range(nsteps):
-            rc = self.lib.oracle_step(_ptrs(self.fields), *self.n, C.byref(params), float(dt))
+            rc = fn(_ptrs(self.fields), *self.n, C.byref(params), float(dt))
             assert rc == 0
 
     def periodic(self) -> None:
@@ -111,14 +128,25 @@ class OracleMesh:
         return self.lib.oracle_reduce(_ptrs(self.fields), len(handles), h, *self.n, int(rtype),
                                       int(normalise))
 
+    def diagnostics(self) -> tuple[float, float, float, float]:
+        """max, min and rms of |u| and rms_exp of lnrho (oracle_diagnostics:
+        OpenMP, long-double sums, RMS normalised as sqrt(sum / N))."""
+        out = (C.c_double * 4)()
+        self.lib.oracle_diagnostics(_ptrs(self.fields), *self.n, out)
+        return tuple(out)
+
     def interior(self, w: int) -> np.ndarray:
         g = abi.NGHOST
         return self.fields[w][g:-g, g:-g, g:-g]
 
 
 # --- the reference's own host utils (optional) ------------------------------
-def ref_lib(prec_name: str):
-    path = os.path.join(ORACLE_DIR, "_ref", f"libref_utils_{prec_name}.so")
+def ref_lib(prec_name: str, build: str = ""):
+    """The reference's host utils: build "" is the bit-exact pinning build
+    (-O3 -march=x86-64-v2 -ffp-contract=off), "avx2" the speed build
+    (-O3 -march=x86-64-v3, GCC's default contraction), used only for timing."""
+    suffix = f"_{build}" if build else ""
+    path = os.path.join(ORACLE_DIR, "_ref", f"libref_utils_{prec_name}{suffix}.so")
     if not os.path.exists(path):
         return None
     prec = abi.PRECISIONS[prec_name]
@@ -135,6 +163,22 @@ def ref_lib(prec_name: str):
     lib.acLoadConfig.restype = C.c_int
     lib.acLoadConfig.argtypes = [C.c_char_p, C.POINTER(abi.info_type(prec))]
     return lib
+
+
+def diagnostics(lnrho, ux, uy, uz):
+    """The standalone's four step diagnostics of interior arrays: max, min and
+    rms of |u| and rms_exp of lnrho, RMS as sqrt(sum / N) (modelreduce.c:76-209
+    with the host normalisation), in double precision with pairwise sums (for
+    candidate states held as arrays; OracleMesh.diagnostics for the oracle's)."""
+    a = np.asarray(ux, dtype=np.float64)
+    b = np.asarray(uy, dtype=np.float64)
+    c = np.asarray(uz, dtype=np.float64)
+    sq = a * a + b * b + c * c
+    ln = np.sqrt(sq)
+    e = np.exp(np.asarray(lnrho, dtype=np.float64))
+    n = sq.size
+    return (float(ln.max()), float(ln.min()), math.sqrt(float(sq.sum()) / n),
+            math.sqrt(float((e * e).sum()) / n))
 
 
 def normwise_error(candidate: np.ndarray, model: np.ndarray) -> float:

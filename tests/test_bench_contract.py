@@ -26,9 +26,14 @@ def test_reference_arm_prints_the_contract_line():
     assert d["impl"] == "reference"
     assert d["unit"] == "cell-updates/s" and d["higher_is_better"] is True
     assert d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 1 and d["n_gpus"] == 1
-    assert d["config"]["workload"].startswith("MHD RK3, 512^3")
+    # the line names the sample it times: 64^3, with a 128^3 sample beside it
+    assert d["config"]["mesh"] == [64, 64, 64] and "64^3 sample" in d["config"]["workload"]
+    assert set(d["config"]["samples"]) == {"64^3", "128^3"}
+    assert d["config"]["samples"]["64^3"]["value"] == pytest.approx(d["value"])
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["sample"]
+    if cb["kind"] == "reference":  # the build flags are stated
+        assert "-O3" in cb["sample"] and "-march=" in cb["sample"]
     assert cb["value"] == pytest.approx(d["value"])
     e = d["e2e"]
     assert e["value"] == pytest.approx(d["value"]) and e["unit"] == d["unit"]
@@ -54,11 +59,14 @@ def test_traffic_and_peak_come_from_committed_files():
 
 
 def test_cpu_oracle_sample_reports_all_cores():
-    """The multi-core CPU figure: the oracle's FP64 solver with OpenMP on every
-    host core, a bounded sample."""
+    """The multi-core CPU figure: the oracle's FP64 solver with OpenMP on the
+    host cores this process may use, a bounded sample; `cores` is the thread
+    count the oracle's OpenMP loops ran with."""
     import bench
+    import oracle_lib as O
 
     r = bench.cpu_oracle_sample(budget_s=0.2, n=16)
     assert r["kind"] == "port" and r["unit"] == bench.UNIT
-    assert r["cores"] == (os.cpu_count() or 1)
+    assert r["cores"] == O.omp_threads()
+    assert r["cpus_available"] == len(os.sched_getaffinity(0))
     assert r["value"] > 0 and "FP64" in r["sample"]
