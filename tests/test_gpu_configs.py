@@ -20,7 +20,8 @@ oracle is itself within 1e-15 of it):
       finiteness only).
 
 Tolerances, normwise per field (max|cand - model| / max|model| over the
-interior) and relative per diagnostic: FP32 1e-5, FP64 1e-12, mixed 1e-6.
+interior) and per diagnostic (relative; min |u| against max |u|): FP32 1e-5,
+FP64 1e-12, mixed 1e-6.
 """
 import math
 
@@ -49,8 +50,15 @@ def interior(a):
     return a[g:-g, g:-g, g:-g]
 
 
-def rel(a, b):
-    return abs(a - b) / abs(b) if b != 0 else abs(a - b)
+def diag_errors(got, want):
+    """Errors of the four diagnostics (max, min, rms of |u|; rms_exp of lnrho):
+    each relative to its own value, except min |u|, which is a tiny number
+    (4e-6 against a max of 5e-3 here) and is measured against max |u|, the
+    scale of the field whose rounding it carries, as the field errors are and as
+    the reference's autotest bounds its errors by the range
+    (samples/standalone/autotest.cc:97-161)."""
+    scale = (want[0], want[0], want[2], want[3])
+    return [abs(g - w) / abs(s) for g, w, s in zip(got, want, scale)]
 
 
 # ---------------------------------------------------------------------------
@@ -106,9 +114,11 @@ def test_256cube_10_steps_with_diagnostics_vs_oracle(flavour, oracle_256):
         dev.synchronize()
         assert dev.status() == 0
         errs = [O.normwise_error(interior(dev.store_double(w)), om.interior(w)) for w in range(8)]
-    derr = [max(rel(g, w) for g, w in zip(gs, ws)) for gs, ws in zip(got, want)]
+    per = [diag_errors(gs, ws) for gs, ws in zip(got, want)]
+    derr = [max(p) for p in per]
     print(flavour, "fields", ["%.2e" % e for e in errs], "diagnostics per step",
-          ["%.1e" % e for e in derr])
+          ["%.1e" % e for e in derr], "worst per diagnostic",
+          ["%.1e" % max(p[q] for p in per) for q in range(4)])
     assert max(errs) <= TOL[flavour], errs
     assert max(derr) <= TOL[flavour], derr
 
