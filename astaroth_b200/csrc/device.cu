@@ -61,6 +61,7 @@ struct StepGraph {
     unsigned long long launches;
     bool ghost[2]; // ghost_ok of both blocks after a replay
     bool lo[2];    // lo_stale of both blocks after a replay
+    bool diag;     // the captured step's last substep folds the step diagnostics
 };
 
 enum { STEP_FIXED = 0, STEP_CFL = 1 };
@@ -108,6 +109,24 @@ struct device_s {
         int nin, handles[3];
         double vals[3]; // MAX, MIN, RMS sum
     } red3;
+
+    // Step diagnostics folded by the last substep's solve launch (enabled by
+    // acDeviceSetStepDiagnostics): max, min and sum of |u|^2 and the sum of
+    // exp(lnrho)^2 of the block it wrote, kept with that block and the epoch
+    // after the launch; a reduction asking for one of them while nothing has
+    // changed reads the record (one copy to the host for all four).
+    bool step_diag;
+    double* diag_partials; // 4 per CTA, diag_max_ctas CTAs
+    int diag_max_ctas;
+    unsigned* diag_counter;
+    double* diag_result;   // 4 doubles
+    double* h_diag;        // pinned, 4 doubles
+    struct {
+        bool valid, fetched;
+        const void* block;
+        unsigned long long epoch;
+        double vals[4];
+    } diag;
 
     double* xfer; // device staging buffer for the double-precision views
     size_t xfer_elems;
@@ -249,9 +268,11 @@ AcResult
 acb_host::prepare_table(const SolveConfig* cfgs, int n)
 {
     for (int c = 0; c < n; ++c)
-        for (int st = 0; st < 7; ++st) {
-            // kern[0..3], then kern_dt[0..2]
-            const void* k = st < 4 ? cfgs[c].kern[st] : cfgs[c].kern_dt[st - 4];
+        for (int st = 0; st < 10; ++st) {
+            // kern[0..3], then kern_dt[0..2], then kern_diag[0..2]
+            const void* k = st < 4   ? cfgs[c].kern[st]
+                            : st < 7 ? cfgs[c].kern_dt[st - 4]
+                                     : cfgs[c].kern_diag[st - 7];
             if (!k)
                 continue;
             ACB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -452,8 +473,18 @@ launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e,
         a.P.rk_beta = kRkBeta[step];
     }
 
-    const SolveKernelFn kern = dt_dev ? (SolveKernelFn)cfg.kern_dt[step]
-                                      : (SolveKernelFn)cfg.kern[step == 2 && d->forcing ? 3 : step];
+    // the last substep over the whole interior folds the step diagnostics
+    // when they are enabled
+    const bool whole = s.x == NGHOST && s.y == NGHOST && s.z == NGHOST &&
+                       e.x == NGHOST + d->L.nx && e.y == NGHOST + d->L.ny &&
+                       e.z == NGHOST + d->L.nz;
+    const bool diag = d->step_diag && step == 2 && whole;
+    SolveKernelFn kern;
+    if (diag)
+        kern = (SolveKernelFn)cfg.kern_diag[dt_dev ? 2 : (d->forcing ? 1 : 0)];
+    else
+        kern = dt_dev ? (SolveKernelFn)cfg.kern_dt[step]
+                      : (SolveKernelFn)cfg.kern[step == 2 && d->forcing ? 3 : step];
     int per_sm = 0;
     ACB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern,
                                                                  cfg.threads, cfg.smem));
@@ -467,10 +498,26 @@ launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e,
     g.nseg  = (g.nzr + g.zseg - 1) / g.zseg;
     g.tasks = ntiles * g.nseg;
     long long grid = std::min(slots, g.tasks);
+    if (diag) {
+        if (grid > d->diag_max_ctas) {
+            fprintf(stderr, "astaroth_b200: %lld CTAs exceed the step diagnostics' %d partials\n",
+                    grid, d->diag_max_ctas);
+            return AC_FAILURE;
+        }
+        a.diag_partials = d->diag_partials;
+        a.diag_counter  = d->diag_counter;
+        a.diag_result   = d->diag_result;
+    }
     kern<<<(unsigned)grid, cfg.threads, cfg.smem, st>>>(d->tmap[d->cur], a, d->cmap[d->cur]);
     ACB_CUDA_CHECK(cudaGetLastError());
     d->launches++;
     d->write_epoch++;
+    if (diag) {
+        d->diag.valid   = true;
+        d->diag.fetched = false;
+        d->diag.block   = d->blk[d->cur ^ 1];
+        d->diag.epoch   = d->write_epoch;
+    }
     d->ghost_ok[d->cur ^ 1] = false; // the out block's ghosts are stale now
     d->lo_stale[d->cur ^ 1] = false; // (all of them, hi and lo alike)
     return AC_SUCCESS;
@@ -580,6 +627,28 @@ run_reduce(const Device d, cudaStream_t st, int rtype, int nin, const int* handl
     if (reduce_args(d, rtype, nin, handles, a, blocks) != AC_SUCCESS)
         return AC_FAILURE;
     const int which  = rtype == RTYPE_MAX ? 0 : (rtype == RTYPE_MIN ? 1 : (rtype == RTYPE_RMS ? 2 : -1));
+    // the step diagnostics the last solve folded, while the block is unchanged
+    const bool is_u = nin == RED_VEC && handles[0] == VTXBUF_UUX && handles[1] == VTXBUF_UUY &&
+                      handles[2] == VTXBUF_UUZ;
+    const int dq = is_u && which >= 0 ? which
+                   : (nin == RED_SCAL && rtype == RTYPE_RMS_EXP && handles[0] == VTXBUF_LNRHO)
+                       ? 3
+                       : -1;
+    if (dq >= 0 && d->diag.valid && d->diag.block == d->blk[d->cur] &&
+        d->diag.epoch == d->write_epoch) {
+        if (!d->diag.fetched) {
+            ACB_CUDA_CHECK(cudaMemcpyAsync(d->h_diag, d->diag_result, 4 * sizeof(double),
+                                           cudaMemcpyDeviceToHost, st));
+            ACB_CUDA_CHECK(cudaStreamSynchronize(st));
+            for (int q = 0; q < 4; ++q)
+                d->diag.vals[q] = d->h_diag[q];
+            d->diag.fetched = true;
+        }
+        // max and min were folded as |u|^2: sqrt is monotonic and correctly
+        // rounded, so this is the max (min) of the lengths a pass would take
+        *result = dq <= 1 ? sqrt(d->diag.vals[dq]) : d->diag.vals[dq];
+        return AC_SUCCESS;
+    }
     if (which >= 0 && (nin == RED_SCAL || nin == RED_VEC)) {
         // MAX, MIN and RMS together: one pass over the fields serves all three
         // requests while the block is unchanged (the diagnostics of a step)
@@ -824,6 +893,7 @@ replay_steps(const Device device, cudaStream_t st, int kind, unsigned long long 
             G.ghost[1]  = device->ghost_ok[1];
             G.lo[0]     = device->lo_stale[0];
             G.lo[1]     = device->lo_stale[1];
+            G.diag      = device->step_diag;
             device->launches = before;
             if (rc != AC_SUCCESS) {
                 cudaGraphDestroy(g);
@@ -842,6 +912,14 @@ replay_steps(const Device device, cudaStream_t st, int kind, unsigned long long 
         device->lo_stale[0] = G.lo[0];
         device->lo_stale[1] = G.lo[1];
         device->cur ^= 1; // three swaps per step
+        if (G.diag) { // the replayed last substep folded the new block's diagnostics
+            device->diag.valid   = true;
+            device->diag.fetched = false;
+            device->diag.block   = device->blk[device->cur];
+            device->diag.epoch   = device->write_epoch;
+        }
+        else
+            device->diag.valid = false;
     }
     return AC_SUCCESS;
 }
@@ -1160,6 +1238,12 @@ acDeviceCreate(const int id, const AcMeshInfo config, Device* device_handle)
     ACB_CUDA_CHECK(cudaMemset(d->red_counter, 0, sizeof(unsigned)));
     ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_result, 3 * sizeof(double)));
     ACB_CUDA_CHECK(cudaMallocHost((void**)&d->h_result, 3 * sizeof(double)));
+    d->diag_max_ctas = d->num_sms * 8;
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->diag_partials, 4 * sizeof(double) * d->diag_max_ctas));
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->diag_counter, sizeof(unsigned)));
+    ACB_CUDA_CHECK(cudaMemset(d->diag_counter, 0, sizeof(unsigned)));
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->diag_result, 4 * sizeof(double)));
+    ACB_CUDA_CHECK(cudaMallocHost((void**)&d->h_diag, 4 * sizeof(double)));
     ACB_CUDA_CHECK(cudaMalloc((void**)&d->status, sizeof(unsigned)));
     ACB_CUDA_CHECK(cudaMemset(d->status, 0, sizeof(unsigned)));
     ACB_CUDA_CHECK(cudaMalloc((void**)&d->cfl, 3 * sizeof(double)));
@@ -1200,6 +1284,10 @@ acDeviceDestroy(Device device)
     cudaFree(device->red_counter);
     cudaFree(device->red_result);
     cudaFreeHost(device->h_result);
+    cudaFree(device->diag_partials);
+    cudaFree(device->diag_counter);
+    cudaFree(device->diag_result);
+    cudaFreeHost(device->h_diag);
     cudaFree(device->status);
     cudaFree(device->cfl);
     if (device->xfer)
@@ -1759,6 +1847,15 @@ acDeviceGetMemoryFootprint(const Device device, size_t* bytes)
     if (device->lo[0])
         b += 2 * block_bytes(device->L);
     *bytes = b;
+    return AC_SUCCESS;
+}
+
+AcResult
+acDeviceSetStepDiagnostics(const Device device, const int enabled)
+{
+    device->step_diag = enabled != 0;
+    device->diag.valid = false;
+    device->uniform_version++; // whole-step graphs are captured again
     return AC_SUCCESS;
 }
 

@@ -42,6 +42,10 @@ struct SolveConfig {
     // single mesh: substeps 0, 1, 2 reading the time step from device memory
     // (null in the ensemble table)
     const void* kern_dt[3];
+    // single mesh, substep 2 also folding the step diagnostics of its output:
+    // plain, with helical forcing, and reading the time step from device memory
+    // (null in the ensemble table)
+    const void* kern_diag[3];
 };
 
 // "tile32x8_ring9", "..._tmacentre" when the centre values are staged by TMA
@@ -75,12 +79,16 @@ make_solve_config()
     if constexpr (ENS) {
         c.kern[3]    = nullptr;
         c.kern_dt[0] = c.kern_dt[1] = c.kern_dt[2] = nullptr;
+        c.kern_diag[0] = c.kern_diag[1] = c.kern_diag[2] = nullptr;
     }
     else {
         c.kern[3]    = (const void*)solve_kernel<Cfg, 3, ENS>;
         c.kern_dt[0] = (const void*)solve_kernel<Cfg, 0, ENS, true>;
         c.kern_dt[1] = (const void*)solve_kernel<Cfg, 1, ENS, true>;
         c.kern_dt[2] = (const void*)solve_kernel<Cfg, 2, ENS, true>;
+        c.kern_diag[0] = (const void*)solve_kernel<Cfg, 2, ENS, false, true>;
+        c.kern_diag[1] = (const void*)solve_kernel<Cfg, 3, ENS, false, true>;
+        c.kern_diag[2] = (const void*)solve_kernel<Cfg, 2, ENS, true, true>;
     }
     return c;
 }

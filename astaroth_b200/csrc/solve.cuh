@@ -104,6 +104,12 @@ struct SolveArgs {
     float* out_lo;   // mixed build: lo parts of `out`
     unsigned* status;
     SolveParams<T> P;
+    // step diagnostics (kernels built with DIAG): four FP64 partials per CTA,
+    // a finishing counter (zero between launches; the last CTA resets it) and
+    // the folded result {max |u|^2, min |u|^2, sum |u|^2, sum exp(lnrho)^2}
+    double* diag_partials;
+    unsigned* diag_counter;
+    double* diag_result;
     // ensemble launches only
     const MemberDesc<T>* members;
     int nmembers;
@@ -147,9 +153,12 @@ struct CentreSet {
     static constexpr bool PREV = STEP > 0;
     static constexpr bool LO   = ACB_MIXED != 0;
     static constexpr int N     = (PREV ? 1 : 0) + (LO ? (PREV ? 2 : 1) : 0);
-    // staged by TMA only where it pays (measured at 512^3): the three arrays of
-    // mixed substeps 1 and 2; one array is cheaper as plain loads
-    static constexpr bool STAGE = N == 3;
+    // staged by TMA in the single-precision builds' configurations with a
+    // centre ring (the mixed build's): the three arrays of substeps 1 and 2
+    // and the lo parts of substep 0, whose plain loads left its warps waiting
+    // on memory (long-scoreboard stalls 1.66 per issued instruction at 256^3;
+    // the 512^3 step 17.43 -> 17.22 ms, same-box A/B)
+    static constexpr bool STAGE = N >= 1;
     // position of each map's array in a centre slot (-1: not loaded)
     static constexpr int POS_PREV    = PREV ? 0 : -1;
     static constexpr int POS_CUR_LO  = LO ? (PREV ? 1 : 0) : -1;
@@ -519,11 +528,15 @@ pair_derivs_q(const F2* __restrict__ c, const int* zo, const PT& P,
     // within 2.2e-7 of FP64.
     // First differences f(+k) - f(-k) directly, as prime_pair forms the queued
     // ones, so results do not depend on where a task's z segment starts.
+    // The difference form is evaluated as S = 2 (f(-k) - f0) + (f(+k) - f(-k)),
+    // one fused multiply-add on the two exact differences (the first
+    // difference is formed anyway): a single rounding of the same value,
+    // three packed operations per point pair instead of four.
     constexpr bool DIFF_FORM = ACB_MIXED != 0;
     auto dsum = [&](F2 p, F2 m, F2& D, F2& S) {
         D = sub2(p, m);
         if constexpr (DIFF_FORM)
-            S = add2(sub2(p, F0), sub2(m, F0));
+            S = fma2(F2{0x4000000040000000ull}, sub2(m, F0), D); // (2, 2) * (m - f0) + D
         else
             S = add2(p, m);
     };
@@ -824,6 +837,36 @@ pair_add2(F2 hi, F2 lo, F2 d, F2& ohi, F2& olo)
 
 } // namespace acb
 
+// Step diagnostics of the output state, accumulated per consumer thread while
+// the last substep writes it: max, min and sum of |u|^2 and sum of
+// exp(lnrho)^2, in FP64 from the stored values (hi + lo in the mixed build),
+// each value formed exactly as the reduction kernels form it (reduce.cuh:
+// red_load, red_len2, the RMS_EXP filter), so max and min equal a separate
+// pass bit for bit (sqrt is monotonic) and the sums differ only in their order.
+struct DiagAcc {
+    double mx, mn, su, se;
+};
+
+__device__ __forceinline__ void
+diag_init(DiagAcc& a)
+{
+    a.mx = -INFINITY;
+    a.mn = INFINITY;
+    a.su = 0.0;
+    a.se = 0.0;
+}
+
+__device__ __forceinline__ void
+diag_add(DiagAcc& a, double lnrho, double ux, double uy, double uz)
+{
+    const double l2 = __fma_rn(uz, uz, __fma_rn(uy, uy, __dmul_rn(ux, ux)));
+    a.mx            = fmax(a.mx, l2);
+    a.mn            = fmin(a.mn, l2);
+    a.su += l2;
+    const double e = exp(lnrho);
+    a.se += e * e;
+}
+
 // Values of the vertex's own column that the update needs besides the ring:
 // the previous state (s > 0) and, in the mixed build, the lo parts.
 // FP64 build: one value per field.
@@ -913,12 +956,13 @@ member_of(const MemberDesc<T>* md, int n, long long t)
 // One task of a consumer warp: the planes of one (tile, z segment) column.
 // Waits for the ring, computes and stores every output plane, releases the
 // slots, and advances the plane counter q. Returns false if the CTA aborts.
-template <class Cfg, int STEP, bool ENS, bool DTDEV, class PT>
+template <class Cfg, int STEP, bool ENS, bool DTDEV, bool DIAG, class PT>
 __device__ __forceinline__ bool
 consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
              long long lt, state_t* out, float* in_lo, float* out_lo, const void* ring,
              uint64_t* full, uint64_t* empty, volatile int* abort_flag, uint32_t& q,
-             const void* centre, uint64_t* full_c, uint64_t* empty_c, uint32_t& oq)
+             const void* centre, uint64_t* full_c, uint64_t* empty_c, uint32_t& oq,
+             DiagAcc& dacc)
 {
     using CS          = CentreSet<STEP>;
     constexpr bool CT = Cfg::NC > 0 && !ENS && CS::STAGE;
@@ -1053,6 +1097,9 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
 #if ACB_MIXED
                 acb::F2* ol2 = reinterpret_cast<acb::F2*>(out_lo);
 #endif
+                // lane 0 of arrays 0..3 holds lnrho, ux, uy, uz: their stored
+                // values for the step diagnostics (hi and, mixed, lo)
+                float dh[ACB_NARR], dl[ACB_NARR];
 #pragma unroll
                 for (int ar = 0; ar < ACB_NARR; ++ar) {
                     const int fa = acb_field(ar, 0), fb = acb_field(ar, 1);
@@ -1072,6 +1119,11 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
                         acb::pair_add2(h2, w2, acb::pk2(fo[ar - 1], 0.f), h2, w2);
                     o2[e]  = h2;
                     ol2[e] = w2;
+                    if constexpr (DIAG) {
+                        float t_;
+                        acb::upk2(h2, dh[ar], t_);
+                        acb::upk2(w2, dl[ar], t_);
+                    }
 #else
                     acb::F2 r;
                     if (STEP == 0)
@@ -1082,9 +1134,28 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
                     if (STEP == 3 && ar >= 1)
                         r = acb::add2(r, acb::pk2(fo[ar - 1], 0.f));
                     o2[e] = r;
+                    if constexpr (DIAG) {
+                        float t_;
+                        acb::upk2(r, dh[ar], t_);
+                        dl[ar] = 0.f;
+                    }
 #endif
                 }
+                if constexpr (DIAG) {
+                    // (double)hi + (double)lo, as the reductions read a value
+                    double v[4];
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) {
+                        v[f] = (double)dh[f];
+#if ACB_MIXED
+                        v[f] += (double)dl[f];
+#endif
+                    }
+                    diag_add(dacc, v[0], v[1], v[2], v[3]);
+                }
                 (void)cur;
+                (void)dh;
+                (void)dl;
             }
             else {
                 // double precision: previous state loaded a plane ahead
@@ -1096,6 +1167,7 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
                 acb::mhd_rhs<T, BX, FIELD>(c, zo, P, roc, cur);
                 if constexpr (STEP == 3)
                     acb::forcing_at<T>(a.P, i, j, k, fo);
+                T dv[4];
 #pragma unroll
                 for (int f = 0; f < ACB_NF; ++f) {
                     T r;
@@ -1106,7 +1178,12 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
                     if (STEP == 3 && f >= 1 && f <= 3)
                         r += fo[f - 1];
                     out[fidx(L, f, id)] = r;
+                    if (f < 4)
+                        dv[f] = r;
                 }
+                if constexpr (DIAG)
+                    diag_add(dacc, (double)dv[0], (double)dv[1], (double)dv[2], (double)dv[3]);
+                (void)dv;
             }
         }
         __syncwarp();
@@ -1142,9 +1219,70 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
 template <bool ENS>
 using SolveKernelArgs = typename std::conditional<ENS, EnsSolveArgs<AcReal>, SolveArgs<AcReal>>::type;
 
+// Folds the consumer threads' step diagnostics: a warp butterfly, the warps
+// in order, one partial per CTA, and the last CTA to finish folds the partials
+// in CTA order into a.diag_result (deterministic; no atomics on data).
+// Every consumer warp reaches it, also after an abort (its waits are bounded).
+template <class Cfg>
+__device__ __forceinline__ void
+diag_finish(const SolveArgs<AcReal>& a, DiagAcc d)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        d.mx = fmax(d.mx, __shfl_xor_sync(0xffffffffu, d.mx, o));
+        d.mn = fmin(d.mn, __shfl_xor_sync(0xffffffffu, d.mn, o));
+        d.su += __shfl_xor_sync(0xffffffffu, d.su, o);
+        d.se += __shfl_xor_sync(0xffffffffu, d.se, o);
+    }
+    __shared__ double wred[Cfg::CWARPS][4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        wred[warp][0] = d.mx;
+        wred[warp][1] = d.mn;
+        wred[warp][2] = d.su;
+        wred[warp][3] = d.se;
+    }
+    // the consumer warps only: the producer warps have left
+    asm volatile("bar.sync 1, %0;" ::"n"(Cfg::CONSUMERS) : "memory");
+    if (threadIdx.x != 0)
+        return;
+    double r[4] = {wred[0][0], wred[0][1], wred[0][2], wred[0][3]};
+    for (int w = 1; w < Cfg::CWARPS; ++w) {
+        r[0] = fmax(r[0], wred[w][0]);
+        r[1] = fmin(r[1], wred[w][1]);
+        r[2] += wred[w][2];
+        r[3] += wred[w][3];
+    }
+    double* p = a.diag_partials + 4 * (size_t)blockIdx.x;
+    p[0]      = r[0];
+    p[1]      = r[1];
+    p[2]      = r[2];
+    p[3]      = r[3];
+    __threadfence();
+    if (atomicAdd(a.diag_counter, 1u) != gridDim.x - 1)
+        return;
+    __threadfence();
+    const volatile double* v = a.diag_partials;
+    double f[4] = {v[0], v[1], v[2], v[3]};
+    for (unsigned b = 1; b < gridDim.x; ++b) {
+        f[0] = fmax(f[0], v[4 * b + 0]);
+        f[1] = fmin(f[1], v[4 * b + 1]);
+        f[2] += v[4 * b + 2];
+        f[3] += v[4 * b + 3];
+    }
+    a.diag_result[0] = f[0];
+    a.diag_result[1] = f[1];
+    a.diag_result[2] = f[2];
+    a.diag_result[3] = f[3];
+    *a.diag_counter  = 0u; // zero for the next launch
+    __threadfence();
+}
+
 // DTDEV: the time step is read from device memory (SolveParams::dt_dev), for
 // steps whose time step the device chooses; single meshes, no forcing.
-template <class Cfg, int STEP, bool ENS, bool DTDEV = false>
+// DIAG: the launch also folds the step diagnostics of its output (diag_finish);
+// single meshes, the last substep over the whole interior.
+template <class Cfg, int STEP, bool ENS, bool DTDEV = false, bool DIAG = false>
 __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     solve_kernel(const __grid_constant__ CUtensorMap tin,
                  const __grid_constant__ SolveKernelArgs<ENS> a,
@@ -1284,6 +1422,8 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
 
     // ---------------------------------------------------------------- consumers
     uint32_t q = 0, oq = 0;
+    DiagAcc dacc;
+    diag_init(dacc);
     for (long long t = blockIdx.x; t < ntasks; t += gridDim.x) {
         bool ok;
         if constexpr (ENS) {
@@ -1293,16 +1433,23 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
             const int m             = member_of(a.members, a.nmembers, tg_);
             const MemberDesc<T>* md = a.members + m;
             const SolveGeom gv      = md->g;
-            ok = consume_task<Cfg, STEP, ENS, DTDEV>(a, gv, a.mp[m], tg_ - md->task_begin, md->out,
-                                              md->in_lo, md->out_lo, ring, full, empty,
-                                              &abort_flag, q, centre, full_c, empty_c, oq);
+            ok = consume_task<Cfg, STEP, ENS, DTDEV, false>(a, gv, a.mp[m], tg_ - md->task_begin,
+                                                     md->out, md->in_lo, md->out_lo, ring, full,
+                                                     empty, &abort_flag, q, centre, full_c,
+                                                     empty_c, oq, dacc);
         }
         else {
-            ok = consume_task<Cfg, STEP, ENS, DTDEV>(a, a.g, a.P, t, a.out, a.in_lo, a.out_lo, ring, full,
-                                              empty, &abort_flag, q, centre, full_c, empty_c,
-                                              oq);
+            ok = consume_task<Cfg, STEP, ENS, DTDEV, DIAG>(a, a.g, a.P, t, a.out, a.in_lo, a.out_lo,
+                                                    ring, full, empty, &abort_flag, q, centre,
+                                                    full_c, empty_c, oq, dacc);
         }
-        if (!ok)
-            return;
+        if (!ok) {
+            if constexpr (DIAG)
+                break; // every consumer warp still reaches the fold
+            else
+                return;
+        }
     }
+    if constexpr (DIAG)
+        diag_finish<Cfg>(a, dacc);
 }

@@ -144,6 +144,10 @@ class Device:
         _check(self.lib.acDeviceSetSimulationTime(self.handle, stream, t),
                "acDeviceSetSimulationTime")
 
+    def set_step_diagnostics(self, enabled: bool) -> None:
+        _check(self.lib.acDeviceSetStepDiagnostics(self.handle, int(bool(enabled))),
+               "acDeviceSetStepDiagnostics")
+
     def set_forcing(self, enabled: bool) -> None:
         _check(self.lib.acDeviceSetForcing(self.handle, int(bool(enabled))), "acDeviceSetForcing")
 

@@ -56,7 +56,7 @@ ASTAROTH_B200_H = [
     "acDeviceGetMemoryFootprint", "acDeviceIntegrateStep", "acDeviceIntegrateSteps",
     "acDeviceIntegrateStepCFL", "acDeviceIntegrateStepsCFL", "acDeviceGetTimestepRecord",
     "acDeviceSetSimulationTime",
-    "acDeviceSetForcing", "acDeviceLoadVertexBufferDouble", "acDeviceStoreVertexBufferDouble",
+    "acDeviceSetStepDiagnostics", "acDeviceSetForcing", "acDeviceLoadVertexBufferDouble", "acDeviceStoreVertexBufferDouble",
     "acDeviceReduceScalDouble", "acDeviceReduceVecDouble", "acReduceScalNoAlloc",
     "acForcingParamsFromUniforms", "acForcingParamsGenerate", "acDeviceLoadForcingParams",
     "acEnsembleCreate", "acEnsembleDestroy", "acEnsembleLoadMember", "acEnsembleStoreMember",
@@ -168,6 +168,7 @@ def _declare(lib: C.CDLL, prec: abi.Precision) -> None:
         "acDeviceGetTimestepRecord": (res, [Dev, i, C.POINTER(R), C.POINTER(C.c_double),
                                             C.POINTER(C.c_ulonglong)]),
         "acDeviceSetSimulationTime": (res, [Dev, i, C.c_double]),
+        "acDeviceSetStepDiagnostics": (res, [Dev, i]),
         "acDeviceSetForcing": (res, [Dev, i]),
         "acDeviceLoadVertexBufferDouble": (res, [Dev, i, i, C.c_void_p]),
         "acDeviceStoreVertexBufferDouble": (res, [Dev, i, i, C.c_void_p]),

@@ -588,6 +588,7 @@ def forced_run(n: int, steps: int, warmup: int, ranks, gpu: int) -> dict:
             del g
             torch.cuda.empty_cache()
         dev.set_forcing(True)
+        dev.set_step_diagnostics(True)  # the four diagnostics folded into substep 2
         gen = ForcingGenerator("mixed", info, seed=5)
         st = torch.cuda.ExternalStream(dev.cuda_stream(0))
         diag = {}
@@ -619,13 +620,28 @@ def forced_run(n: int, steps: int, warmup: int, ranks, gpu: int) -> dict:
         wall_ms = (time.perf_counter() - t0) * 1e3
         ranks.barrier()
         ms = ranks.max(e0.elapsed_time(e1))
+        # the same steps without reading the diagnostics: their share of a step
+        def bare():
+            dev.load_forcing_params(gen.next())
+            dev.integrate_step(dt)
+
+        dev.synchronize()
+        ranks.barrier()
+        e0.record(st)
+        for _ in range(steps):
+            bare()
+        e1.record(st)
+        e1.synchronize()
+        bare_ms = ranks.max(e0.elapsed_time(e1))
         cells = n ** 3
         return {"mesh": [n, n, n], "steps": steps, "warmup": warmup,
                 "ms_per_step": ms / steps, "wall_ms_per_step": wall_ms / steps,
+                "ms_per_step_without_diagnostics": bare_ms / steps,
+                "diagnostics_share_of_step": (ms - bare_ms) / ms,
                 "cell_updates_per_s": ranks.world * cells * steps / (ms * 1e-3),
                 "device_state_gb": footprint / 1e9, "free_gb_before": free_b / 1e9, "dt": dt,
                 "step": "forcing params load + 3 x (ghost fill + forced solve) + 4 FP64 "
-                        "reductions read back",
+                        "diagnostics read back (folded into the last substep's solve)",
                 "forcing": "helical, |k| in [1, 3], magnitude 0.05, relhel 0, seed 5",
                 "last_step_diagnostics": {"umax": diag["umax"], "umin": diag["umin"],
                                           "urms": math.sqrt(diag["urms_sum"] / cells),
@@ -650,7 +666,10 @@ def diagnostics_run(n: int, steps: int, warmup: int, ranks, gpu: int,
     from astaroth_b200 import Device, abi
 
     out = {"mesh": [n, n, n], "steps": steps, "warmup": warmup, "init": "seeded 1e-3 noise",
-           "diagnostics": "max, min, rms of |u|; rms_exp of lnrho; each read back"}
+           "diagnostics": "max, min, rms of |u|; rms_exp of lnrho; each read back",
+           "folded": "acDeviceSetStepDiagnostics: the last substep folds the four; "
+                     "diagnostics_share_of_step = (step + diagnostics, folded) / step alone - 1 "
+                     "as a share of the former"}
     if check_steps > 0:
         out["errors_vs_oracle"] = diagnostics_errors(n, check_steps, gpu)
     for flav in ("sp", "dp"):
@@ -682,10 +701,21 @@ def diagnostics_run(n: int, steps: int, warmup: int, ranks, gpu: int,
             step_ms = timed(lambda: dev.integrate_step(DT), steps)
             both_ms = timed(lambda: (dev.integrate_step(DT), diag()), steps)
             red_ms = timed(diag, steps) / 4
+            # the same with the diagnostics folded into the last substep
+            dev.set_step_diagnostics(True)
+            fold_step_ms = timed(lambda: dev.integrate_step(DT), steps)
+            fold_both_ms = timed(lambda: (dev.integrate_step(DT), diag()), steps)
+            dev.set_step_diagnostics(False)
             out[flav] = {"ms_per_step": step_ms, "ms_per_step_with_diagnostics": both_ms,
                          "ms_per_reduction": red_ms,
                          "cell_updates_per_s_with_diagnostics":
-                             ranks.world * n ** 3 / (both_ms * 1e-3)}
+                             ranks.world * n ** 3 / (both_ms * 1e-3),
+                         "folded": {"ms_per_step": fold_step_ms,
+                                    "ms_per_step_with_diagnostics": fold_both_ms,
+                                    "diagnostics_share_of_step":
+                                        (fold_both_ms - step_ms) / fold_both_ms,
+                                    "cell_updates_per_s_with_diagnostics":
+                                        ranks.world * n ** 3 / (fold_both_ms * 1e-3)}}
         finally:
             dev.destroy()
             del host

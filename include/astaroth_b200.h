@@ -98,6 +98,20 @@ AcResult acDeviceGetTimestepRecord(const Device device, const Stream stream, AcR
  * Synchronises `stream`. */
 AcResult acDeviceSetSimulationTime(const Device device, const Stream stream, const double time);
 
+/* Step diagnostics folded into the last substep (no counterpart in the
+ * reference, whose standalone runs separate reductions after each step,
+ * samples/standalone/simulation.cc:250-310). When enabled, every substep 2 over
+ * the whole interior (acDeviceIntegrateSubstep, acDeviceIntegrateStep(s), the
+ * CFL steps, forced or not) also accumulates, over the state it writes, max,
+ * min and sum of |u|^2 and sum of exp(lnrho)^2 in FP64. Until that block
+ * changes, acDeviceReduceVec(MAX | MIN | RMS, UUX, UUY, UUZ) and
+ * acDeviceReduceScal(RMS_EXP, LNRHO) (and their Double, Node and Legacy forms)
+ * return these instead of reading the fields again: the first of them copies
+ * all four to the host (one synchronisation), the others return at once. MAX
+ * and MIN equal a separate reduction bit for bit; the sums differ from one by
+ * their summation order only. Off by default. */
+AcResult acDeviceSetStepDiagnostics(const Device device, const int enabled);
+
 /* Enables the helical forcing term at the last substep
  * (acc/mhd_solver/stencil_kernel.ac:611-648,713-717; off in the reference's
  * shipped module). Its parameters are the AC_forcing_* / AC_k_force* /
