@@ -10,11 +10,9 @@
 
 // Solve tile shapes (tile width, tile height, ring depth, CTAs per SM hint)
 #if AC_DOUBLE_PRECISION == 1
-// two consumer threads per column (groups A and B): 8 consumer warps and a
-// producer warpgroup for 128-column tiles, 4 consumer warps for 64 columns
-using SolveCfg0 = TileCfg<32, 4, 7, 1, 2>;
-using SolveCfg1 = TileCfg<16, 8, 7, 1, 2>;
-using SolveCfg2 = TileCfg<32, 2, 8, 1, 2>;
+using SolveCfg0 = TileCfg<32, 4, 8, 1>;
+using SolveCfg1 = TileCfg<16, 8, 8, 1>;
+using SolveCfg2 = TileCfg<32, 2, 10, 2>;
 #elif ACB_MIXED
 // all three stage the centre values of substeps 1 and 2 by TMA; the first (the
 // default, 12 consumer warps) is the fastest on the 512^3 workload
@@ -74,8 +72,7 @@ make_solve_config()
     c.threads = Cfg::THREADS;
     c.launch_regs = Cfg::REG_LAUNCH;
     c.NC          = ENS ? 0 : Cfg::NC;
-    // ensembles load the centre values directly: no centre ring
-    c.smem    = ENS ? Cfg::ring_bytes() + Cfg::exchange_bytes() : Cfg::smem_bytes();
+    c.smem    = ENS ? Cfg::ring_bytes() : Cfg::smem_bytes(); // ensembles load centres directly
     c.kern[0] = (const void*)solve_kernel<Cfg, 0, ENS>;
     c.kern[1] = (const void*)solve_kernel<Cfg, 1, ENS>;
     c.kern[2] = (const void*)solve_kernel<Cfg, 2, ENS>;

@@ -177,20 +177,15 @@ struct TileCfg {
     static constexpr int NC = NC_;
     static constexpr int CENTRE = TX_ * TY_ * ACB_NARR; // elements of one centre array set
     static constexpr int BX = TX_ + 8, BY = TY_ + 6;
-    // double precision: two consumer threads per column, in two groups of
-    // warps (group A: lnrho, ux, uy, uz; group B: ax, ay, az, ss)
-    static constexpr bool SPLIT    = sizeof(state_t) == 8;
-    static constexpr int COLUMNS   = TX_ * TY_;
-    static constexpr int CONSUMERS = (SPLIT ? 2 : 1) * COLUMNS; // threads on the columns
+    static constexpr int CONSUMERS = TX_ * TY_;        // one thread per (x, y) column
     static constexpr int CWARPS    = CONSUMERS / 32;   // consumer warps
-    static_assert(COLUMNS % 32 == 0, "a tile's columns fill whole warps");
-    // 8 or 12 consumer warps: the producer is a whole warpgroup (4 warps, one
-    // of them working) that hands its registers to the consumers (setmaxnreg),
-    // so each consumer thread gets the registers its z queues need. An SM
-    // sub-partition's 16K registers hold 2 consumer warps and 1 producer warp
-    // (2 * 232 + 40 = 504 <= 512 registers a lane), or 3 and 1
-    // (3 * 160 + 32 = 512): more warps to hide latency, fewer registers.
-    static constexpr bool WGSPEC = CWARPS == 8 || CWARPS == 12;
+    // Single precision with 8 or 12 consumer warps: the producer is a whole
+    // warpgroup (4 warps, one of them working) that hands its registers to the
+    // consumers (setmaxnreg), so each consumer thread gets the registers its z
+    // queues need. An SM sub-partition's 16K registers hold 2 consumer warps
+    // and 1 producer warp (2 * 232 + 40 = 504 <= 512 registers a lane), or 3
+    // and 1 (3 * 160 + 32 = 512): more warps to hide latency, fewer registers.
+    static constexpr bool WGSPEC = sizeof(state_t) == 4 && (CWARPS == 8 || CWARPS == 12);
     static constexpr int THREADS = CONSUMERS + (WGSPEC ? 128 : 32); // plus the producer
     static constexpr int REG_CONSUMER = CWARPS == 12 ? 160 : 232;
     static constexpr int REG_PRODUCER = CWARPS == 12 ? 32 : 40;
@@ -204,17 +199,13 @@ struct TileCfg {
     {
         return (size_t)(ACB_MIXED ? 3 : 1) * CENTRE * ACB_ELEM;
     }
-    // the two groups' exchange (double precision): two buffers of 11 + 3
-    // doubles per column
-    static constexpr size_t exchange_bytes() { return SPLIT ? (size_t)2 * 14 * COLUMNS * 8 : 0; }
-    static constexpr size_t smem_bytes()
-    {
-        return ring_bytes() + NC * centre_slot_bytes() + exchange_bytes();
-    }
+    static constexpr size_t smem_bytes() { return ring_bytes() + NC * centre_slot_bytes(); }
     // A task starts once the first 2 NGHOST planes are in the ring (the queue
-    // priming and the first output plane's upper half): a shallower ring could
-    // never hold them.
-    static_assert(NP >= 2 * NGHOST, "ring too shallow for the planes a task waits for");
+    // priming and the first output plane's upper half), and without queues an
+    // output plane needs all 2 NGHOST + 1 of its planes at once: a shallower
+    // ring could never hold them.
+    static_assert(NP >= (sizeof(state_t) == 4 ? 2 * NGHOST : 2 * NGHOST + 1),
+                  "ring too shallow for the planes a task waits for");
     static_assert(smem_bytes() <= 227 * 1024, "shared memory of one CTA exceeded");
 };
 
@@ -786,258 +777,6 @@ rhs_terms(const FieldDerivs<T>& lr, const FieldDerivs<T>& ux, const FieldDerivs<
     roc[7]     = -(u0 * ss.gx + u1 * ss.gy + u2 * ss.gz) + inv_pT * heat + hc;
 }
 
-// ---- double precision: two consumer groups per column ----------------------
-// A column's eight fields are split between two consumer threads: group A
-// forms the derivatives of lnrho, ux, uy, uz and group B those of ax, ay, az, ss,
-// each with z register queues for its four fields (the same 2.5D scheme as the
-// single-precision pairs, in scalar FP64), so only the centre plane and the
-// three above it are read from the ring. One exchange through shared memory per
-// plane joins them: B sends B = curl A, j, s, grad s and lap s; A sends u. A then
-// evaluates continuity, momentum and entropy, B the induction equation.
-
-// z queue of one double-precision field: values at z-1, z-2, z-3 and the
-// running sums of the lower halves of its xz / yz diagonals (see PairQ)
-struct DQ {
-    double v1, v2, v3;
-    double xa1, xa2, xa3;
-    double ya1, ya2, ya3;
-};
-
-__device__ __forceinline__ void
-dzacc_push(double& a1, double& a2, double& a3, const double* e, double d1, double d2, double d3)
-{
-    a1 = __fma_rn(e[0], d1, a2);
-    a2 = __fma_rn(e[1], d2, a3);
-    a3 = __dmul_rn(e[2], d3);
-}
-
-__device__ __forceinline__ double
-dzacc_upper(const double* e, double u1, double u2, double u3)
-{
-    return __fma_rn(e[2], u3, __fma_rn(e[1], u2, __dmul_rn(e[0], u1)));
-}
-
-// lower-half sums of a z diagonal at the first plane of a task, from the three
-// planes below it; the rounding sequence of dzacc_push, so a task's priming
-// equals what streaming would have built
-__device__ __forceinline__ void
-dzacc_prime(const double* __restrict__ c, const int* zo, int step, const double* e, double& a1,
-            double& a2, double& a3)
-{
-    auto d = [&](int plane, int k) { return c[zo[plane] + k * step] - c[zo[plane] - k * step]; };
-    const double t3 = __dmul_rn(e[2], d(0, 3));
-    const double b2 = __fma_rn(e[1], d(1, 2), t3);
-    const double b3 = __dmul_rn(e[2], d(1, 3));
-    a1              = __fma_rn(e[0], d(2, 1), b2);
-    a2              = __fma_rn(e[1], d(2, 2), b3);
-    a3              = __dmul_rn(e[2], d(2, 3));
-}
-
-template <int BX, class F, class PT>
-__device__ __forceinline__ void
-dprime(const double* __restrict__ c, const int* zo, const PT& P, DQ& Q)
-{
-    Q.v1 = c[zo[2]];
-    Q.v2 = c[zo[1]];
-    Q.v3 = c[zo[0]];
-    if (F::XZ)
-        dzacc_prime(c, zo, 1, P.cx[1], Q.xa1, Q.xa2, Q.xa3);
-    if (F::YZ)
-        dzacc_prime(c, zo, BX, P.cx[2], Q.ya1, Q.ya2, Q.ya3);
-}
-
-// sum_k c_k d_k, k = 1..3, in a fixed rounding sequence
-__device__ __forceinline__ double
-dsum3(const double* cf, double d1, double d2, double d3)
-{
-    return __fma_rn(cf[2], d3, __fma_rn(cf[1], d2, __dmul_rn(cf[0], d1)));
-}
-
-// c0 f0 + sum_k c_k s_k
-__device__ __forceinline__ double
-dsum4(const double* cf, double f0, double s1, double s2, double s3)
-{
-    return __fma_rn(cf[3], s3, __fma_rn(cf[2], s2, __fma_rn(cf[1], s1, __dmul_rn(cf[0], f0))));
-}
-
-// All derivatives of one FP64 field at the thread's vertex: x, y pencils and
-// the xy diagonal from the centre plane, the z pencil's upper half and the
-// z diagonals' upper halves from the three planes above (zo[4..6]), their
-// lower halves from the queue, which then advances by one plane.
-template <int BX, class F, class PT>
-__device__ __forceinline__ FieldDerivs<double>
-dfield_q(const double* __restrict__ c, const int* zo, const PT& P, DQ& Q)
-{
-    FieldDerivs<double> r;
-    const double f0 = c[0];
-    r.v             = f0;
-    double DX[3], DY[3];
-    {
-        double S[3];
-#pragma unroll
-        for (int k = 1; k <= 3; ++k) {
-            const double p = c[k], m = c[-k];
-            DX[k - 1] = p - m;
-            S[k - 1]  = p + m;
-        }
-        if (F::GX)
-            r.gx = dsum3(P.c1[0], DX[0], DX[1], DX[2]);
-        r.xx = dsum4(P.c2[0], f0, S[0], S[1], S[2]);
-    }
-    {
-        double S[3];
-#pragma unroll
-        for (int k = 1; k <= 3; ++k) {
-            const double p = c[k * BX], m = c[-k * BX];
-            DY[k - 1] = p - m;
-            S[k - 1]  = p + m;
-        }
-        if (F::GY)
-            r.gy = dsum3(P.c1[1], DY[0], DY[1], DY[2]);
-        r.yy = dsum4(P.c2[1], f0, S[0], S[1], S[2]);
-    }
-    {
-        const double p1 = c[zo[4]], p2 = c[zo[5]], p3 = c[zo[6]];
-        if (F::GZ)
-            r.gz = dsum3(P.c1[2], p1 - Q.v1, p2 - Q.v2, p3 - Q.v3);
-        r.zz = dsum4(P.c2[2], f0, p1 + Q.v1, p2 + Q.v2, p3 + Q.v3);
-    }
-    if (F::XY) {
-        double E[3];
-#pragma unroll
-        for (int k = 1; k <= 3; ++k)
-            E[k - 1] = (c[k + k * BX] + c[-k - k * BX]) - (c[k - k * BX] + c[-k + k * BX]);
-        r.xy = dsum3(P.cx[0], E[0], E[1], E[2]);
-    }
-    if (F::XZ) {
-        double u[3];
-#pragma unroll
-        for (int k = 1; k <= 3; ++k)
-            u[k - 1] = c[zo[3 + k] + k] - c[zo[3 + k] - k];
-        r.xz = dzacc_upper(P.cx[1], u[0], u[1], u[2]) - Q.xa1;
-        dzacc_push(Q.xa1, Q.xa2, Q.xa3, P.cx[1], DX[0], DX[1], DX[2]);
-    }
-    if (F::YZ) {
-        double u[3];
-#pragma unroll
-        for (int k = 1; k <= 3; ++k)
-            u[k - 1] = c[zo[3 + k] + k * BX] - c[zo[3 + k] - k * BX];
-        r.yz = dzacc_upper(P.cx[2], u[0], u[1], u[2]) - Q.ya1;
-        dzacc_push(Q.ya1, Q.ya2, Q.ya3, P.cx[2], DY[0], DY[1], DY[2]);
-    }
-    Q.v3 = Q.v2;
-    Q.v2 = Q.v1;
-    Q.v1 = f0;
-    return r;
-}
-
-// What group B sends group A: B = curl A, j, s, grad s, lap s (11 values);
-// what A sends B: u (3 values).
-constexpr int DX_B = 11, DX_A = 3;
-
-// Group B before the exchange: B and j from the derivatives of A.
-template <class PT>
-__device__ __forceinline__ void
-group_b_fields(const FieldDerivs<double>& ax, const FieldDerivs<double>& ay,
-               const FieldDerivs<double>& az, const FieldDerivs<double>& ss, const PT& P,
-               double out[DX_B], double lapA[3])
-{
-    const double B0 = az.gy - ay.gz;
-    const double B1 = ax.gz - az.gx;
-    const double B2 = ay.gx - ax.gy;
-    lapA[0]         = ax.xx + ax.yy + ax.zz;
-    lapA[1]         = ay.xx + ay.yy + ay.zz;
-    lapA[2]         = az.xx + az.yy + az.zz;
-    out[0]          = B0;
-    out[1]          = B1;
-    out[2]          = B2;
-    out[3]          = P.inv_mu0 * ((ax.xx + ay.xy + az.xz) - lapA[0]);
-    out[4]          = P.inv_mu0 * ((ax.xy + ay.yy + az.yz) - lapA[1]);
-    out[5]          = P.inv_mu0 * ((ax.xz + ay.yz + az.zz) - lapA[2]);
-    out[6]          = ss.v;
-    out[7]          = ss.gx;
-    out[8]          = ss.gy;
-    out[9]          = ss.gz;
-    out[10]         = ss.xx + ss.yy + ss.zz;
-}
-
-// Group B after the exchange: induction, u x B + eta lap(A).
-template <class PT>
-__device__ __forceinline__ void
-group_b_rhs(const double b[DX_B], const double lapA[3], const double u[DX_A], const PT& P,
-            double roc[3])
-{
-    roc[0] = (u[1] * b[2] - u[2] * b[1]) + P.eta * lapA[0];
-    roc[1] = (u[2] * b[0] - u[0] * b[2]) + P.eta * lapA[1];
-    roc[2] = (u[0] * b[1] - u[1] * b[0]) + P.eta * lapA[2];
-}
-
-// Group A after the exchange: continuity, momentum and entropy
-// (stencil_kernel.ac:355-403,483-528, the terms of rhs_terms).
-// roc: lnrho, ux, uy, uz, ss.
-template <class PT>
-__device__ __forceinline__ void
-group_a_rhs(const FieldDerivs<double>& lr, const FieldDerivs<double>& ux,
-            const FieldDerivs<double>& uy, const FieldDerivs<double>& uz, const double b[DX_B],
-            const PT& P, double roc[5])
-{
-    typedef double T;
-    const T u0 = ux.v, u1 = uy.v, u2 = uz.v;
-    const T divu = ux.gx + uy.gy + uz.gz;
-    roc[0]       = -(u0 * lr.gx + u1 * lr.gy + u2 * lr.gz) - divu;
-    const T B0 = b[0], B1 = b[1], B2 = b[2], j0 = b[3], j1 = b[4], j2 = b[5];
-    const T ssv = b[6], sgx = b[7], sgy = b[8], sgz = b[9], lap_s = b[10];
-
-    const T third = (T)1 / (T)3, twothird = (T)2 / (T)3, half = (T)0.5;
-    const T S00   = twothird * ux.gx - third * (uy.gy + uz.gz);
-    const T S11   = twothird * uy.gy - third * (ux.gx + uz.gz);
-    const T S22   = twothird * uz.gz - third * (ux.gx + uy.gy);
-    const T S01   = half * (ux.gy + uy.gx);
-    const T S02   = half * (ux.gz + uz.gx);
-    const T S12   = half * (uy.gz + uz.gy);
-
-    const T E       = P.gamma * ssv * P.inv_cp + P.gm1 * (lr.v - P.lnrho0);
-    const T expE    = rexp<T>(E);
-    const T cs2     = P.cs2_sound * expE;
-    const T rho     = rexp<T>(lr.v);
-    const T inv_rho = rrcp<T>(rho);
-
-    const T gd0  = ux.xx + uy.xy + uz.xz;
-    const T gd1  = ux.xy + uy.yy + uz.yz;
-    const T gd2  = ux.xz + uy.yz + uz.zz;
-    const T jxB0 = j1 * B2 - j2 * B1;
-    const T jxB1 = j2 * B0 - j0 * B2;
-    const T jxB2 = j0 * B1 - j1 * B0;
-    const T lapu0 = ux.xx + ux.yy + ux.zz;
-    const T lapu1 = uy.xx + uy.yy + uy.zz;
-    const T lapu2 = uz.xx + uz.yy + uz.zz;
-    const T Sg0   = S00 * lr.gx + S01 * lr.gy + S02 * lr.gz;
-    const T Sg1   = S01 * lr.gx + S11 * lr.gy + S12 * lr.gz;
-    const T Sg2   = S02 * lr.gx + S12 * lr.gy + S22 * lr.gz;
-    roc[1] = -(ux.gx * u0 + ux.gy * u1 + ux.gz * u2) - cs2 * (P.inv_cp * sgx + lr.gx) +
-             inv_rho * jxB0 + P.nu * (lapu0 + third * gd0 + (T)2 * Sg0) + P.zeta * gd0;
-    roc[2] = -(uy.gx * u0 + uy.gy * u1 + uy.gz * u2) - cs2 * (P.inv_cp * sgy + lr.gy) +
-             inv_rho * jxB1 + P.nu * (lapu1 + third * gd1 + (T)2 * Sg1) + P.zeta * gd1;
-    roc[3] = -(uz.gx * u0 + uz.gy * u1 + uz.gz * u2) - cs2 * (P.inv_cp * sgz + lr.gz) +
-             inv_rho * jxB2 + P.nu * (lapu2 + third * gd2 + (T)2 * Sg2) + P.zeta * gd2;
-
-    const T inv_pT = rrcp<T>(rho * (P.exp_lnT0 * expE));
-    const T SS = S00 * S00 + S01 * S01 + S02 * S02 + S01 * S01 + S11 * S11 + S12 * S12 +
-                 S02 * S02 + S12 * S12 + S22 * S22;
-    const T heat = P.eta_mu0 * (j0 * j0 + j1 * j1 + j2 * j2) + (T)2 * rho * P.nu * SS +
-                   P.zeta * rho * divu * divu;
-    const T lap_lr = lr.xx + lr.yy + lr.zz;
-    const T first  = P.gamma_inv_cp * lap_s + P.gm1 * lap_lr;
-    const T sec0   = P.gamma_inv_cp * sgx + P.gm1 * lr.gx;
-    const T sec1   = P.gamma_inv_cp * sgy + P.gm1 * lr.gy;
-    const T sec2   = P.gamma_inv_cp * sgz + P.gm1 * lr.gz;
-    const T thi0   = P.gamma * (P.inv_cp * sgx + lr.gx) - lr.gx;
-    const T thi1   = P.gamma * (P.inv_cp * sgy + lr.gy) - lr.gy;
-    const T thi2   = P.gamma * (P.inv_cp * sgz + lr.gz) - lr.gz;
-    const T hc = P.k_heat * inv_rho * (first + (sec0 * thi0 + sec1 * thi1 + sec2 * thi2));
-    roc[4]     = -(u0 * sgx + u1 * sgy + u2 * sgz) + inv_pT * heat + hc;
-}
-
 // Helical forcing at interior vertex (i, j, k) (stencil_kernel.ac:611-648 with
 // a single device: global index = local index, global grid = local grid).
 template <typename T>
@@ -1467,258 +1206,6 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
     return true;
 }
 
-// One task of the two-group double-precision consumers (Cfg::SPLIT): as
-// consume_task with the z queues, each column's fields split between group A
-// (lnrho, ux, uy, uz; it also updates ss) and group B (ax, ay, az), and one
-// exchange per plane through xbuf (two buffers of 11 + 3 doubles per column,
-// struct-of-arrays) guarded by xbar[2] (one arrival per consumer warp, bounded
-// waits). A buffer is written again two planes later, after every warp's
-// arrival at the plane between has shown that it finished reading it.
-// The previous state (s > 0) of single meshes arrives by TMA in the centre ring
-// (read after the exchange, so it holds no registers through the stencils);
-// ensemble members load it a plane ahead.
-template <class Cfg, int STEP, bool ENS, bool DTDEV, bool DIAG, class PT>
-__device__ __forceinline__ bool
-consume_task_split(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P, long long lt,
-                   state_t* out, const void* ring, uint64_t* full, uint64_t* empty,
-                   volatile int* abort_flag, uint32_t& q, const void* centre, uint64_t* full_c,
-                   uint64_t* empty_c, uint32_t& oq, double* xbuf, uint64_t* xbar, uint32_t& xq,
-                   DiagAcc& dacc)
-{
-    using T  = AcReal;
-    using CS = CentreSet<STEP>;
-    constexpr bool CT = Cfg::NC > 0 && !ENS && CS::STAGE;
-    using acb::DFlags;
-    constexpr int TX = Cfg::TX, NP = Cfg::NP, BX = Cfg::BX;
-    constexpr int FIELD = Cfg::FIELD, PLANE = Cfg::PLANE, COLS = Cfg::COLUMNS;
-    constexpr int NB = acb::DX_B, NA = acb::DX_A;
-    const int tid   = threadIdx.x;
-    const int lane  = tid & 31;
-    const int grp   = tid / COLS; // warp-uniform: COLS is a multiple of 32
-    const int cidx  = tid - grp * COLS;
-    const int tx    = cidx % TX;
-    const int ty    = cidx / TX;
-    const Layout& L = gv.L;
-    const TaskGeom<Cfg> tg(gv, lt, (long long)gv.ntx * gv.nty);
-    const int nload = tg.nout + 2 * NGHOST;
-    const int i     = tg.i0 + tx;
-    const int j     = tg.j0 + ty;
-    const bool act  = (i >= gv.start.x) && (i < gv.end.x) && (j < gv.end.y);
-    const T rkA     = a.P.rkA;
-    T rkB           = a.P.rkB;
-    if constexpr (DTDEV)
-        rkB = (T)(a.P.rk_beta * *a.P.dt_dev);
-    const int col = (ty + NGHOST) * BX + (tx + 4);
-
-    bool ok = true;
-    for (int l = 0; l < 2 * NGHOST && ok; ++l)
-        ok = mbar_wait_bounded(&full[(q + l) % NP], ((q + l) / NP) & 1u);
-    ok = __all_sync(0xffffffffu, ok);
-
-    acb::DQ Q[4];
-    if (ok && act) {
-        const uint32_t sc = (q + NGHOST) % NP;
-        int zo[7];
-#pragma unroll
-        for (int dz = -NGHOST; dz <= NGHOST; ++dz)
-            zo[dz + NGHOST] = ((int)((q + NGHOST + dz) % NP) - (int)sc) * PLANE;
-        const double* c = reinterpret_cast<const double*>(ring) + (size_t)sc * PLANE + col;
-        if (grp == 0) {
-            acb::dprime<BX, DFlags<ACB_D_LNRHO>>(c + 0 * FIELD, zo, P, Q[0]);
-            acb::dprime<BX, DFlags<ACB_D_UUX>>(c + 1 * FIELD, zo, P, Q[1]);
-            acb::dprime<BX, DFlags<ACB_D_UUY>>(c + 2 * FIELD, zo, P, Q[2]);
-            acb::dprime<BX, DFlags<ACB_D_UUZ>>(c + 3 * FIELD, zo, P, Q[3]);
-        }
-        else {
-            acb::dprime<BX, DFlags<ACB_D_AX>>(c + 4 * FIELD, zo, P, Q[0]);
-            acb::dprime<BX, DFlags<ACB_D_AY>>(c + 5 * FIELD, zo, P, Q[1]);
-            acb::dprime<BX, DFlags<ACB_D_AZ>>(c + 6 * FIELD, zo, P, Q[2]);
-            acb::dprime<BX, DFlags<ACB_D_SS>>(c + 7 * FIELD, zo, P, Q[3]);
-        }
-    }
-    // the three planes below the first output plane now live in the queues
-    __syncwarp();
-    if (lane == 0 && ok)
-        for (int l = 0; l < NGHOST; ++l)
-            mbar_arrive(&empty[(q + l) % NP]);
-
-    // previous state of the fields this thread updates, a plane ahead:
-    // group A lnrho, ux, uy, uz, ss; group B ax, ay, az
-    constexpr int NV = 5;
-    T pv_next[NV] = {0, 0, 0, 0, 0};
-    auto load_prev = [&](long long id, T* pv) {
-        if constexpr (STEP > 0) {
-            if (grp == 0) {
-#pragma unroll
-                for (int n = 0; n < 4; ++n)
-                    pv[n] = out[fidx(L, n, id)];
-                pv[4] = out[fidx(L, 7, id)];
-            }
-            else {
-#pragma unroll
-                for (int n = 0; n < 3; ++n)
-                    pv[n] = out[fidx(L, 4 + n, id)];
-            }
-        }
-    };
-    if (!CT && act)
-        load_prev(lidx(L, i, j, tg.k0), pv_next);
-
-    for (int p = 0; p < tg.nout; ++p) {
-        if (ok) {
-            const uint32_t l = q + p + 2 * NGHOST;
-            ok = mbar_wait_bounded(&full[l % NP], (l / NP) & 1u);
-            ok = __all_sync(0xffffffffu, ok);
-        }
-        if constexpr (CT) {
-            if (ok) {
-                ok = mbar_wait_bounded(&full_c[oq % Cfg::NC], (oq / Cfg::NC) & 1u);
-                ok = __all_sync(0xffffffffu, ok);
-            }
-        }
-        if (!ok || *abort_flag) {
-            if (lane == 0) {
-                atomicOr(a.status, (unsigned)ACB_STATUS_TMA_TIMEOUT);
-                *abort_flag = 1;
-            }
-            return false;
-        }
-        const int k          = tg.k0 + p;
-        const long long id   = lidx(L, i, j, k);
-        const uint32_t sc    = (q + p + NGHOST) % NP;
-        int zo[7];
-#pragma unroll
-        for (int dz = 0; dz <= NGHOST; ++dz)
-            zo[dz + NGHOST] = ((int)((q + p + NGHOST + dz) % NP) - (int)sc) * PLANE;
-        const double* c = reinterpret_cast<const double*>(ring) + (size_t)sc * PLANE + col;
-        T pv[NV];
-#pragma unroll
-        for (int n = 0; n < NV; ++n)
-            pv[n] = pv_next[n];
-        if (!CT && act && p + 1 < tg.nout)
-            load_prev(id + L.plane, pv_next);
-        // this plane's exchange buffer: B's values [NB][COLS], then A's [NA][COLS]
-        double* xb = xbuf + (size_t)(xq & 1u) * (NB + NA) * COLS;
-        acb::FieldDerivs<double> f0, f1, f2, f3;
-        double bv[NB], lapA[3];
-        if (act) {
-            if (grp == 0) {
-                f0 = acb::dfield_q<BX, DFlags<ACB_D_LNRHO>>(c + 0 * FIELD, zo, P, Q[0]);
-                f1 = acb::dfield_q<BX, DFlags<ACB_D_UUX>>(c + 1 * FIELD, zo, P, Q[1]);
-                f2 = acb::dfield_q<BX, DFlags<ACB_D_UUY>>(c + 2 * FIELD, zo, P, Q[2]);
-                f3 = acb::dfield_q<BX, DFlags<ACB_D_UUZ>>(c + 3 * FIELD, zo, P, Q[3]);
-                xb[(NB + 0) * COLS + cidx] = f1.v;
-                xb[(NB + 1) * COLS + cidx] = f2.v;
-                xb[(NB + 2) * COLS + cidx] = f3.v;
-            }
-            else {
-                f0 = acb::dfield_q<BX, DFlags<ACB_D_AX>>(c + 4 * FIELD, zo, P, Q[0]);
-                f1 = acb::dfield_q<BX, DFlags<ACB_D_AY>>(c + 5 * FIELD, zo, P, Q[1]);
-                f2 = acb::dfield_q<BX, DFlags<ACB_D_AZ>>(c + 6 * FIELD, zo, P, Q[2]);
-                f3 = acb::dfield_q<BX, DFlags<ACB_D_SS>>(c + 7 * FIELD, zo, P, Q[3]);
-                acb::group_b_fields(f0, f1, f2, f3, P, bv, lapA);
-#pragma unroll
-                for (int n = 0; n < NB; ++n)
-                    xb[n * COLS + cidx] = bv[n];
-            }
-        }
-        // the exchange: every consumer warp arrives, then waits for the others
-        __syncwarp();
-        if (lane == 0)
-            mbar_arrive(&xbar[xq & 1u]);
-        ok = mbar_wait_bounded(&xbar[xq & 1u], (xq >> 1) & 1u);
-        ok = __all_sync(0xffffffffu, ok);
-        ++xq;
-        if (!ok) {
-            if (lane == 0) {
-                atomicOr(a.status, (unsigned)ACB_STATUS_TMA_TIMEOUT);
-                *abort_flag = 1;
-            }
-            return false;
-        }
-        if (CT && act && STEP > 0) {
-            // this output plane's previous state from the centre slot:
-            // [array][TY][TX] doubles
-            const double* cs = reinterpret_cast<const double*>(centre) +
-                               (size_t)(oq % Cfg::NC) * (Cfg::centre_slot_bytes() / 8) + cidx;
-            constexpr int FS = Cfg::COLUMNS;
-            if (grp == 0) {
-#pragma unroll
-                for (int n = 0; n < 4; ++n)
-                    pv[n] = cs[n * FS];
-                pv[4] = cs[7 * FS];
-            }
-            else {
-#pragma unroll
-                for (int n = 0; n < 3; ++n)
-                    pv[n] = cs[(4 + n) * FS];
-            }
-        }
-        if (act) {
-            if (grp == 0) {
-                double b[NB];
-#pragma unroll
-                for (int n = 0; n < NB; ++n)
-                    b[n] = xb[n * COLS + cidx];
-                double roc[5];
-                acb::group_a_rhs(f0, f1, f2, f3, b, P, roc);
-                T fo[3] = {0, 0, 0};
-                if constexpr (STEP == 3)
-                    acb::forcing_at<T>(a.P, i, j, k, fo);
-                const T cur[5]   = {f0.v, f1.v, f2.v, f3.v, b[6]};
-                const int fld[5] = {0, 1, 2, 3, 7};
-                T r5[5];
-#pragma unroll
-                for (int n = 0; n < 5; ++n) {
-                    T r;
-                    if (STEP == 0)
-                        r = cur[n] + rkB * roc[n];
-                    else
-                        r = cur[n] + rkA * (cur[n] - pv[n]) + rkB * roc[n];
-                    if (STEP == 3 && n >= 1 && n <= 3)
-                        r += fo[n - 1];
-                    out[fidx(L, fld[n], id)] = r;
-                    r5[n]                    = r;
-                }
-                if constexpr (DIAG)
-                    diag_add(dacc, (double)r5[0], (double)r5[1], (double)r5[2], (double)r5[3]);
-            }
-            else {
-                const double u[NA] = {xb[(NB + 0) * COLS + cidx], xb[(NB + 1) * COLS + cidx],
-                                      xb[(NB + 2) * COLS + cidx]};
-                double roc[3];
-                acb::group_b_rhs(bv, lapA, u, P, roc);
-                const T cur[3] = {f0.v, f1.v, f2.v};
-#pragma unroll
-                for (int n = 0; n < 3; ++n) {
-                    T r;
-                    if (STEP == 0)
-                        r = cur[n] + rkB * roc[n];
-                    else
-                        r = cur[n] + rkA * (cur[n] - pv[n]) + rkB * roc[n];
-                    out[fidx(L, 4 + n, id)] = r;
-                }
-            }
-        }
-        __syncwarp();
-        // the centre plane is done with (the queues hold what is still needed)
-        if (lane == 0)
-            mbar_arrive(&empty[(q + p + NGHOST) % NP]);
-        if constexpr (CT) {
-            if (lane == 0)
-                mbar_arrive(&empty_c[oq % Cfg::NC]);
-            ++oq;
-        }
-    }
-    // the planes of the task not released yet
-    __syncwarp();
-    if (lane == 0)
-        for (int l = tg.nout + NGHOST; l < nload; ++l)
-            mbar_arrive(&empty[(q + l) % NP]);
-    q += nload;
-    return true;
-}
-
 // Warp-specialised pipeline. Warp CWARPS is the producer: one lane issues one
 // TMA load per plane (all 8 fields of the halo'd tile) into a ring of NP
 // slots, each guarded by a `full` barrier (transaction bytes) and an `empty`
@@ -1819,11 +1306,6 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     __shared__ __align__(8) uint64_t empty_c[NCS];
     unsigned char* centre = smem_raw + Cfg::ring_bytes(); // NC slots of centre_slot_bytes
     __shared__ volatile int abort_flag;
-    // the two consumer groups' exchange (double precision)
-    __shared__ __align__(8) uint64_t xbar[2];
-    // (after the centre ring, which ensemble launches do not allocate)
-    double* xbuf = reinterpret_cast<double*>(smem_raw + Cfg::ring_bytes() +
-                                             (ENS ? 0 : Cfg::NC * Cfg::centre_slot_bytes()));
 
     const int tid  = threadIdx.x;
     const int warp = tid >> 5;
@@ -1836,10 +1318,6 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
         for (int s = 0; s < NCS; ++s) {
             mbar_init(&full_c[s], 1);
             mbar_init(&empty_c[s], CWARPS);
-        }
-        if constexpr (Cfg::SPLIT) {
-            mbar_init(&xbar[0], CWARPS);
-            mbar_init(&xbar[1], CWARPS);
         }
         fence_barrier_init();
         abort_flag = 0;
@@ -1943,7 +1421,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
     }
 
     // ---------------------------------------------------------------- consumers
-    uint32_t q = 0, oq = 0, xq = 0;
+    uint32_t q = 0, oq = 0;
     DiagAcc dacc;
     diag_init(dacc);
     for (long long t = blockIdx.x; t < ntasks; t += gridDim.x) {
@@ -1955,25 +1433,15 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
             const int m             = member_of(a.members, a.nmembers, tg_);
             const MemberDesc<T>* md = a.members + m;
             const SolveGeom gv      = md->g;
-            if constexpr (Cfg::SPLIT)
-                ok = consume_task_split<Cfg, STEP, ENS, DTDEV, false>(
-                    a, gv, a.mp[m], tg_ - md->task_begin, md->out, ring, full, empty,
-                    &abort_flag, q, centre, full_c, empty_c, oq, xbuf, xbar, xq, dacc);
-            else
-                ok = consume_task<Cfg, STEP, ENS, DTDEV, false>(
-                    a, gv, a.mp[m], tg_ - md->task_begin, md->out, md->in_lo, md->out_lo, ring,
-                    full, empty, &abort_flag, q, centre, full_c, empty_c, oq, dacc);
+            ok = consume_task<Cfg, STEP, ENS, DTDEV, false>(a, gv, a.mp[m], tg_ - md->task_begin,
+                                                     md->out, md->in_lo, md->out_lo, ring, full,
+                                                     empty, &abort_flag, q, centre, full_c,
+                                                     empty_c, oq, dacc);
         }
         else {
-            if constexpr (Cfg::SPLIT)
-                ok = consume_task_split<Cfg, STEP, ENS, DTDEV, DIAG>(
-                    a, a.g, a.P, t, a.out, ring, full, empty, &abort_flag, q, centre, full_c,
-                    empty_c, oq, xbuf, xbar, xq, dacc);
-            else
-                ok = consume_task<Cfg, STEP, ENS, DTDEV, DIAG>(a, a.g, a.P, t, a.out, a.in_lo,
-                                                               a.out_lo, ring, full, empty,
-                                                               &abort_flag, q, centre, full_c,
-                                                               empty_c, oq, dacc);
+            ok = consume_task<Cfg, STEP, ENS, DTDEV, DIAG>(a, a.g, a.P, t, a.out, a.in_lo, a.out_lo,
+                                                    ring, full, empty, &abort_flag, q, centre,
+                                                    full_c, empty_c, oq, dacc);
         }
         if (!ok) {
             if constexpr (DIAG)
