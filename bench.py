@@ -58,6 +58,9 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="mesh size (default 512)")
+    ap.add_argument("--flavour", choices=["mixed", "sp", "dp"], default="mixed",
+                    help="library of the measured arm (default mixed; the others for "
+                         "profiling their kernels with the same driver)")
     ap.add_argument("--no-variants", action="store_true", help="skip the FP64/FP32 side runs")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -910,8 +913,9 @@ def run_ours(args) -> None:
     gpu = ranks.local
     torch.cuda.set_device(gpu)
     n = args.n
-    host = host_mesh("mixed", n)
-    dev = Device("mixed", host.info, gpu)
+    arm = args.flavour  # the measured library (the mixed build unless asked)
+    host = host_mesh(arm, n)
+    dev = Device(arm, host.info, gpu)
     tile_config = dev.solve_config()[2]  # the library's default tile configuration
     dev.load_mesh(host)
     res = timed_steps(dev, args.steps, args.warmup, ranks, sample_clocks=True, gpu_index=gpu)
@@ -919,7 +923,7 @@ def run_ours(args) -> None:
 
     # roofline of the dominant kernel (the fused solve): algorithmic bytes per
     # launch over the average launch time from the events around every launch
-    alg = alg_bytes_per_step("mixed", n)
+    alg = alg_bytes_per_step(arm, n)
     achieved_gbs = alg * args.steps / (res["solve_ms_total"] * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
     # DRAM bytes of one s = 1 launch at this size, from the committed ncu
@@ -1007,7 +1011,7 @@ def run_ours(args) -> None:
                 "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak,
                              "unit": "GB/s", "frac": achieved_gbs / peak,
                              "traffic": traffic, "peak_source": peak_kind,
-                             "kernel": f"solve_kernel (mixed, {tile_config})",
+                             "kernel": f"solve_kernel ({arm}, {tile_config})",
                              "alg_bytes_per_cell_step": alg // n ** 3,
                              "solve_ms_per_substep": res["solve_ms_per_substep"]},
                 "clocks": res["clocks"], "gpu_launches": res["launches"],
