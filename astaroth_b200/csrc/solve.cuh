@@ -1221,8 +1221,9 @@ using SolveKernelArgs = typename std::conditional<ENS, EnsSolveArgs<AcReal>, Sol
 
 // Folds the consumer threads' step diagnostics: a warp butterfly, the warps
 // in order, one partial per CTA, and the last CTA to finish folds the partials
-// in CTA order into a.diag_result (deterministic; no atomics on data).
-// Every consumer warp reaches it, also after an abort (its waits are bounded).
+// (its first warp: lane l takes CTAs l, l + 32, ... in order, then a fixed
+// butterfly) into a.diag_result. Deterministic; no atomics on data. Every
+// consumer warp reaches it, also after an abort (its waits are bounded).
 template <class Cfg>
 __device__ __forceinline__ void
 diag_finish(const SolveArgs<AcReal>& a, DiagAcc d)
@@ -1235,6 +1236,7 @@ diag_finish(const SolveArgs<AcReal>& a, DiagAcc d)
         d.se += __shfl_xor_sync(0xffffffffu, d.se, o);
     }
     __shared__ double wred[Cfg::CWARPS][4];
+    __shared__ int dlast;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) {
         wred[warp][0] = d.mx;
@@ -1244,38 +1246,49 @@ diag_finish(const SolveArgs<AcReal>& a, DiagAcc d)
     }
     // the consumer warps only: the producer warps have left
     asm volatile("bar.sync 1, %0;" ::"n"(Cfg::CONSUMERS) : "memory");
-    if (threadIdx.x != 0)
-        return;
-    double r[4] = {wred[0][0], wred[0][1], wred[0][2], wred[0][3]};
-    for (int w = 1; w < Cfg::CWARPS; ++w) {
-        r[0] = fmax(r[0], wred[w][0]);
-        r[1] = fmin(r[1], wred[w][1]);
-        r[2] += wred[w][2];
-        r[3] += wred[w][3];
+    if (threadIdx.x == 0) {
+        double r[4] = {wred[0][0], wred[0][1], wred[0][2], wred[0][3]};
+        for (int w = 1; w < Cfg::CWARPS; ++w) {
+            r[0] = fmax(r[0], wred[w][0]);
+            r[1] = fmin(r[1], wred[w][1]);
+            r[2] += wred[w][2];
+            r[3] += wred[w][3];
+        }
+        double* p = a.diag_partials + 4 * (size_t)blockIdx.x;
+        p[0]      = r[0];
+        p[1]      = r[1];
+        p[2]      = r[2];
+        p[3]      = r[3];
+        __threadfence();
+        dlast = atomicAdd(a.diag_counter, 1u) == gridDim.x - 1;
     }
-    double* p = a.diag_partials + 4 * (size_t)blockIdx.x;
-    p[0]      = r[0];
-    p[1]      = r[1];
-    p[2]      = r[2];
-    p[3]      = r[3];
-    __threadfence();
-    if (atomicAdd(a.diag_counter, 1u) != gridDim.x - 1)
+    asm volatile("bar.sync 1, %0;" ::"n"(Cfg::CONSUMERS) : "memory");
+    if (!dlast || warp != 0)
         return;
     __threadfence();
     const volatile double* v = a.diag_partials;
-    double f[4] = {v[0], v[1], v[2], v[3]};
-    for (unsigned b = 1; b < gridDim.x; ++b) {
-        f[0] = fmax(f[0], v[4 * b + 0]);
-        f[1] = fmin(f[1], v[4 * b + 1]);
-        f[2] += v[4 * b + 2];
-        f[3] += v[4 * b + 3];
+    double f0 = -INFINITY, f1 = INFINITY, f2 = 0.0, f3 = 0.0;
+    for (unsigned b = lane; b < gridDim.x; b += 32) {
+        f0 = fmax(f0, v[4 * b + 0]);
+        f1 = fmin(f1, v[4 * b + 1]);
+        f2 += v[4 * b + 2];
+        f3 += v[4 * b + 3];
     }
-    a.diag_result[0] = f[0];
-    a.diag_result[1] = f[1];
-    a.diag_result[2] = f[2];
-    a.diag_result[3] = f[3];
-    *a.diag_counter  = 0u; // zero for the next launch
-    __threadfence();
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        f0 = fmax(f0, __shfl_xor_sync(0xffffffffu, f0, o));
+        f1 = fmin(f1, __shfl_xor_sync(0xffffffffu, f1, o));
+        f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+        f3 += __shfl_xor_sync(0xffffffffu, f3, o);
+    }
+    if (lane == 0) {
+        a.diag_result[0] = f0;
+        a.diag_result[1] = f1;
+        a.diag_result[2] = f2;
+        a.diag_result[3] = f3;
+        *a.diag_counter  = 0u; // zero for the next launch
+        __threadfence();
+    }
 }
 
 // DTDEV: the time step is read from device memory (SolveParams::dt_dev), for
