@@ -65,6 +65,18 @@ acb_field(int a, int l)
     return ACB_PAIRED ? (l == 0 ? a : (a == 0 ? 7 : a + 3)) : a;
 }
 
+// Mixed build: the lo parts of a block are stored in bfloat16. A pair array's
+// two lo values (A, B) form one 32-bit bf16x2 word, and two pair arrays share an
+// 8-byte element: lo array 0 holds (lnrho, ss) | (ux, ax), lo array 1 holds
+// (uy, ay) | (uz, az), low word first. The lo block thus has ACB_LO_NARR arrays
+// with the hi block's geometry (row pitch, offsets, array stride) and half its
+// bytes. The state (hi, lo) keeps 24 + 8 significant bits plus the sign of lo:
+// storing lo rounds it by at most 2^-9 of itself, at most 2^-34 of hi, far below
+// the single-precision stencils' rounding.
+typedef unsigned short lo16_t;
+static constexpr int ACB_LO_NARR = 2; // lo arrays of a block
+static constexpr int ACB_LO_STEP = 4; // bf16 values per 8-byte element
+
 struct Layout {
     int mx, my, mz;    // logical extents (n + 6)
     int nx, ny, nz;    // interior extents
@@ -114,6 +126,40 @@ __host__ __device__ __forceinline__ long long
 fidx(const Layout& L, int f, long long id)
 {
     return ((long long)acb_array(f) * L.fstride + id) * ACB_LANES + acb_lane(f);
+}
+
+// bytes of one lo block (mixed build)
+static inline size_t
+lo_block_bytes(const Layout& L)
+{
+    return (size_t)L.fstride * ACB_LO_NARR * ACB_ELEM;
+}
+
+// The lo part of field f in a lo block, as bf16 values: the field's lo at
+// vertex element id (lidx) is lo_field(...)[id * ACB_LO_STEP]. Null for a
+// null block (builds without lo parts).
+__host__ __device__ __forceinline__ lo16_t*
+lo_field(lo16_t* lo_block, const Layout& L, int f)
+{
+    if (!lo_block)
+        return nullptr;
+    const int a = acb_array(f);
+    return lo_block + (long long)(a >> 1) * L.fstride * ACB_LO_STEP + (a & 1) * 2 + acb_lane(f);
+}
+
+__device__ __forceinline__ float
+lo16_to_float(lo16_t h)
+{
+    return __uint_as_float((uint32_t)h << 16);
+}
+
+// round to nearest even
+__device__ __forceinline__ lo16_t
+float_to_lo16(float f)
+{
+    unsigned short r;
+    asm("cvt.rn.bf16.f32 %0, %1;" : "=h"(r) : "f"(f));
+    return r;
 }
 
 // Status bits a kernel may raise in the per-device status word.

@@ -75,7 +75,7 @@ struct device_s {
 
     Layout L;
     state_t* blk[2]; // the two field blocks; blk[cur] is `in`
-    float* lo[2];    // mixed build: lo parts of the blocks
+    lo16_t* lo[2];   // mixed build: lo blocks (bf16, see common.cuh)
     int cur;
     // ghost_ok[b]: block b's ghost zone holds the periodic images of its
     // interior (set by a full-box fill of all fields; cleared by any write to
@@ -216,7 +216,7 @@ acb_host::encode_block_map(const Layout& L, const state_t* block, const SolveCon
 
 AcResult
 acb_host::encode_centre_map(const Layout& L, const void* block, const SolveConfig& cfg,
-                            CUtensorMap* map)
+                            CUtensorMap* map, int narr)
 {
     PFN_encodeTiled_t enc = get_encode_tiled();
     if (!enc) {
@@ -224,10 +224,11 @@ acb_host::encode_centre_map(const Layout& L, const void* block, const SolveConfi
         return AC_FAILURE;
     }
     const cuuint64_t esz     = ACB_ELEM;
-    const cuuint64_t dim[4]  = {(cuuint64_t)L.mxp, (cuuint64_t)L.my, (cuuint64_t)L.mz, ACB_NARR};
+    const cuuint64_t dim[4]  = {(cuuint64_t)L.mxp, (cuuint64_t)L.my, (cuuint64_t)L.mz,
+                               (cuuint64_t)narr};
     const cuuint64_t str[3]  = {(cuuint64_t)L.mxp * esz, (cuuint64_t)L.plane * esz,
                                (cuuint64_t)L.fstride * esz};
-    const cuuint32_t box[4]  = {(cuuint32_t)cfg.TX, (cuuint32_t)cfg.TY, 1, ACB_NARR};
+    const cuuint32_t box[4]  = {(cuuint32_t)cfg.TX, (cuuint32_t)cfg.TY, 1, (cuuint32_t)narr};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(block), dim, str,
                      box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -253,10 +254,11 @@ ensure_maps(const Device d)
     memset(d->cmap, 0, sizeof(d->cmap));
     if (cfg.NC > 0) {
         for (int p = 0; p < 2; ++p) {
-            if (encode_centre_map(d->L, d->blk[p ^ 1], cfg, &d->cmap[p].m[0]) != AC_SUCCESS)
+            if (encode_centre_map(d->L, d->blk[p ^ 1], cfg, &d->cmap[p].m[0], ACB_NARR) != AC_SUCCESS)
                 return AC_FAILURE;
-            if (d->lo[p] && (encode_centre_map(d->L, d->lo[p], cfg, &d->cmap[p].m[1]) != AC_SUCCESS ||
-                             encode_centre_map(d->L, d->lo[p ^ 1], cfg, &d->cmap[p].m[2]) != AC_SUCCESS))
+            if (d->lo[p] &&
+                (encode_centre_map(d->L, d->lo[p], cfg, &d->cmap[p].m[1], ACB_LO_NARR) != AC_SUCCESS ||
+                 encode_centre_map(d->L, d->lo[p ^ 1], cfg, &d->cmap[p].m[2], ACB_LO_NARR) != AC_SUCCESS))
                 return AC_FAILURE;
         }
     }
@@ -532,11 +534,11 @@ ensure_lo_ghosts(const Device d, cudaStream_t st, int b)
     if (!d->lo[b] || !d->lo_stale[b])
         return AC_SUCCESS;
     const Layout& L       = d->L;
-    const long long units = halo_units(L);
+    const long long units = halo_units(L, ACB_LO_NARR);
     const int blocks =
         (int)std::max(1LL, std::min((units + 255) / 256, (long long)d->num_sms * 32));
-    halo_full_kernel<<<blocks, 256, 0, st>>>(L, reinterpret_cast<state_t*>(d->lo[b]), nullptr,
-                                             (unsigned)halo_units_a(L), (unsigned)units);
+    halo_full_kernel<<<blocks, 256, 0, st>>>(L, d->lo[b], (unsigned)halo_units_a(L, ACB_LO_NARR),
+                                             (unsigned)units, ACB_LO_NARR);
     ACB_CUDA_CHECK(cudaGetLastError());
     d->launches++;
     d->lo_stale[b] = false;
@@ -563,8 +565,8 @@ launch_halo(const Device d, cudaStream_t st, int3 s, int3 e, int f0, int f1)
         const long long units = halo_units(L);
         const long long want  = (units + 255) / 256;
         const int blocks = (int)std::max(1LL, std::min(want, (long long)d->num_sms * 32));
-        halo_full_kernel<<<blocks, 256, 0, st>>>(L, d->blk[d->cur], nullptr,
-                                                 (unsigned)halo_units_a(L), (unsigned)units);
+        halo_full_kernel<<<blocks, 256, 0, st>>>(L, d->blk[d->cur], (unsigned)halo_units_a(L),
+                                                 (unsigned)units, ACB_NARR);
         ACB_CUDA_CHECK(cudaGetLastError());
         d->launches++;
         d->ghost_ok[d->cur] = true;
@@ -603,7 +605,7 @@ reduce_args(const Device d, int rtype, int nin, const int* handles, ReduceArgs& 
         if (handles[w] < 0 || handles[w] >= NUM_VTXBUF_HANDLES)
             return AC_FAILURE;
         a.f[w]  = d->blk[d->cur] + fidx(L, handles[w], 0);
-        a.lo[w] = d->lo[d->cur] ? d->lo[d->cur] + fidx(L, handles[w], 0) : nullptr;
+        a.lo[w] = lo_field(d->lo[d->cur], L, handles[w]);
     }
     a.nin      = nin;
     a.rtype    = rtype;
@@ -698,15 +700,15 @@ flat_to_elem(const Layout& L, unsigned long long idx)
 // reference order, starting at flat index s, from a staging buffer into the
 // padded layout (and zeroes their lo parts when given: fresh values carry none).
 __global__ void
-scatter_rows_kernel(const Layout L, state_t* __restrict__ field, float* __restrict__ lo,
+scatter_rows_kernel(const Layout L, state_t* __restrict__ field, lo16_t* __restrict__ lo,
                     const state_t* __restrict__ flat, unsigned long long s, unsigned long long n)
 {
     for (unsigned long long u = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; u < n;
          u += (unsigned long long)gridDim.x * blockDim.x) {
-        const long long dev = flat_to_elem(L, s + u) * ACB_LANES;
-        field[dev]          = flat[u];
+        const long long e = flat_to_elem(L, s + u);
+        field[e * ACB_LANES] = flat[u];
         if (lo)
-            lo[dev] = 0.f;
+            lo[e * ACB_LO_STEP] = 0;
     }
 }
 
@@ -746,7 +748,7 @@ acb_host::stage_destroy(StageBuf* stage)
 
 AcResult
 acb_host::copy_field_range(cudaStream_t st, const Layout& L, state_t* field, size_t s,
-                           AcReal* host, size_t count, bool h2d, float* lo_field,
+                           AcReal* host, size_t count, bool h2d, lo16_t* lo_field,
                            StageBuf* stage)
 {
     const size_t w     = sizeof(state_t);
@@ -796,7 +798,7 @@ acb_host::copy_field_range(cudaStream_t st, const Layout& L, state_t* field, siz
 
 // flat (reference-order) double <-> padded field, for the double views and fills
 __global__ void
-pack_kernel(const Layout L, state_t* __restrict__ field, float* __restrict__ lo,
+pack_kernel(const Layout L, state_t* __restrict__ field, lo16_t* __restrict__ lo,
             double* __restrict__ flat, int to_flat, int fill, double value)
 {
     const long long total = (long long)L.mx * L.my * L.mz;
@@ -804,11 +806,12 @@ pack_kernel(const Layout L, state_t* __restrict__ field, float* __restrict__ lo,
          t += (long long)gridDim.x * blockDim.x) {
         const long long row = t / L.mx;
         const int i         = (int)(t - row * L.mx);
-        const long long id  = (L.offx + row * L.mxp + i) * ACB_LANES;
+        const long long e   = L.offx + row * L.mxp + i; // element index
+        const long long id  = e * ACB_LANES;
         if (to_flat) {
             double v = (double)field[id];
             if (ACB_MIXED && lo)
-                v += (double)lo[id];
+                v += (double)lo16_to_float(lo[e * ACB_LO_STEP]);
             flat[t] = v;
         }
         else {
@@ -816,7 +819,7 @@ pack_kernel(const Layout L, state_t* __restrict__ field, float* __restrict__ lo,
             const state_t h = (state_t)v;
             field[id]       = h;
             if (ACB_MIXED && lo)
-                lo[id] = (float)(v - (double)h);
+                lo[e * ACB_LO_STEP] = float_to_lo16((float)(v - (double)h));
         }
     }
 }
@@ -829,7 +832,7 @@ launch_pack(const Device d, cudaStream_t st, int blk, int handle, double* flat, 
     if (ensure_lo_ghosts(d, st, blk) != AC_SUCCESS)
         return AC_FAILURE;
     state_t* f      = d->blk[blk] + fidx(L, handle, 0);
-    float* lo       = d->lo[blk] ? d->lo[blk] + fidx(L, handle, 0) : nullptr;
+    lo16_t* lo      = lo_field(d->lo[blk], L, handle);
     pack_kernel<<<d->num_sms * 8, 256, 0, st>>>(L, f, lo, flat, to_flat, fill, value);
     ACB_CUDA_CHECK(cudaGetLastError());
     d->launches++;
@@ -1228,8 +1231,8 @@ acDeviceCreate(const int id, const AcMeshInfo config, Device* device_handle)
         ACB_CUDA_CHECK(cudaMalloc((void**)&d->blk[b], bytes));
         ACB_CUDA_CHECK(cudaMemset(d->blk[b], 0, bytes));
 #if ACB_MIXED
-        ACB_CUDA_CHECK(cudaMalloc((void**)&d->lo[b], block_bytes(d->L)));
-        ACB_CUDA_CHECK(cudaMemset(d->lo[b], 0, block_bytes(d->L)));
+        ACB_CUDA_CHECK(cudaMalloc((void**)&d->lo[b], lo_block_bytes(d->L)));
+        ACB_CUDA_CHECK(cudaMemset(d->lo[b], 0, lo_block_bytes(d->L)));
 #endif
     }
     d->red_max_blocks = d->num_sms * 8;
@@ -1371,7 +1374,7 @@ acDeviceLoadVertexBufferWithOffset(const Device device, const Stream stream,
     const size_t sidx = acVertexBufferIdx(src.x, src.y, src.z, host_mesh.info);
     const size_t didx = acVertexBufferIdx(dst.x, dst.y, dst.z, device->local_config);
     const Layout& L   = device->L;
-    float* lo         = device->lo[device->cur] ? device->lo[device->cur] + fidx(L, h, 0) : nullptr;
+    lo16_t* lo        = lo_field(device->lo[device->cur], L, h);
     device->ghost_ok[device->cur] = false;
     device->write_epoch++;
     if (ensure_lo_ghosts(device, stream_of(device, stream), device->cur) != AC_SUCCESS)
@@ -1479,19 +1482,19 @@ acDeviceStoreMesh(const Device device, const Stream stream, AcMesh* host_mesh)
 
 // device-to-device flat-range copy between two padded layouts
 __global__ void
-transfer_kernel(const Layout Ls, const state_t* __restrict__ src, const float* __restrict__ slo,
-                long long s0, const Layout Ld, state_t* __restrict__ dst, float* __restrict__ dlo,
+transfer_kernel(const Layout Ls, const state_t* __restrict__ src, const lo16_t* __restrict__ slo,
+                long long s0, const Layout Ld, state_t* __restrict__ dst, lo16_t* __restrict__ dlo,
                 long long d0, long long count)
 {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
          t += (long long)gridDim.x * blockDim.x) {
         const long long a = s0 + t, b = d0 + t;
         const long long ra = a / Ls.mx, rb = b / Ld.mx;
-        const long long ia = (Ls.offx + ra * Ls.mxp + (a - ra * Ls.mx)) * ACB_LANES;
-        const long long ib = (Ld.offx + rb * Ld.mxp + (b - rb * Ld.mx)) * ACB_LANES;
-        dst[ib]            = src[ia];
-        if (ACB_MIXED && dlo)
-            dlo[ib] = slo ? slo[ia] : 0.f; // the (hi, lo) pair moves whole
+        const long long ea = Ls.offx + ra * Ls.mxp + (a - ra * Ls.mx); // element indices
+        const long long eb = Ld.offx + rb * Ld.mxp + (b - rb * Ld.mx);
+        dst[eb * ACB_LANES] = src[ea * ACB_LANES];
+        if (ACB_MIXED && dlo) // the (hi, lo) pair moves whole
+            dlo[eb * ACB_LO_STEP] = slo ? slo[ea * ACB_LO_STEP] : (lo16_t)0;
     }
 }
 
@@ -1519,12 +1522,8 @@ acDeviceTransferVertexBufferWithOffset(const Device src_device, const Stream str
     if (ensure_lo_ghosts(src_device, tst, src_device->cur) != AC_SUCCESS ||
         ensure_lo_ghosts(dst_device, tst, dst_device->cur) != AC_SUCCESS)
         return AC_FAILURE;
-    const float* slo = src_device->lo[src_device->cur]
-                           ? src_device->lo[src_device->cur] + fidx(src_device->L, h, 0)
-                           : nullptr;
-    float* dlo = dst_device->lo[dst_device->cur]
-                     ? dst_device->lo[dst_device->cur] + fidx(dst_device->L, h, 0)
-                     : nullptr;
+    const lo16_t* slo = lo_field(src_device->lo[src_device->cur], src_device->L, h);
+    lo16_t* dlo       = lo_field(dst_device->lo[dst_device->cur], dst_device->L, h);
     transfer_kernel<<<src_device->num_sms * 4, 256, 0, tst>>>(
         src_device->L, src_device->blk[src_device->cur] + fidx(src_device->L, h, 0), slo,
         (long long)sidx, dst_device->L, dst_device->blk[dst_device->cur] + fidx(dst_device->L, h, 0),
@@ -1845,7 +1844,7 @@ acDeviceGetMemoryFootprint(const Device device, size_t* bytes)
 {
     size_t b = 2 * block_bytes(device->L);
     if (device->lo[0])
-        b += 2 * block_bytes(device->L);
+        b += 2 * lo_block_bytes(device->L);
     *bytes = b;
     return AC_SUCCESS;
 }

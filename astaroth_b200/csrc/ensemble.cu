@@ -55,7 +55,7 @@ struct Member {
     AcMeshInfo uniforms; // defaults of the module overlaid with the member's valid values
     Layout L;
     state_t* blk[2];
-    float* lo[2];
+    lo16_t* lo[2]; // mixed build: lo blocks (bf16, see common.cuh)
 };
 
 bool
@@ -238,7 +238,6 @@ build_tables(Ensemble e)
                 e->h_mp[pos] = member_params(make_params(mb.uniforms, L, 0, 0));
             H[pos].L          = L;
             H[pos].block      = mb.blk[p];
-            H[pos].lo         = nullptr; // lo parts of ghosts: never read in an ensemble
             H[pos].unit_begin = units;
             H[pos].units_a    = (unsigned)halo_units_a(L);
             units += halo_units(L);
@@ -421,7 +420,7 @@ acEnsembleCreate(const int device_id, const int num_members, const AcMeshInfo* c
             ACB_CUDA_CHECK(cudaMalloc((void**)&mb.blk[b], bytes));
             ACB_CUDA_CHECK(cudaMemset(mb.blk[b], 0, bytes));
 #if ACB_MIXED
-            const size_t lb = block_bytes(mb.L);
+            const size_t lb = lo_block_bytes(mb.L);
             ACB_CUDA_CHECK(cudaMalloc((void**)&mb.lo[b], lb));
             ACB_CUDA_CHECK(cudaMemset(mb.lo[b], 0, lb));
 #endif
@@ -490,7 +489,7 @@ acEnsembleLoadMember(Ensemble e, const int member, const AcMesh host_mesh)
     }
     e->ghost_ok[e->cur] = false;
     for (int f = 0; f < NUM_VTXBUF_HANDLES; ++f) {
-        float* lo = mb.lo[e->cur] ? mb.lo[e->cur] + fidx(mb.L, f, 0) : nullptr;
+        lo16_t* lo = lo_field(mb.lo[e->cur], mb.L, f);
         if (copy_field_range(e->stream, mb.L, mb.blk[e->cur] + fidx(mb.L, f, 0), 0,
                              host_mesh.vertex_buffer[f], n, true, lo, &e->stage) != AC_SUCCESS)
             return AC_FAILURE;

@@ -22,9 +22,9 @@
 // double), whatever the fields.
 // A thread never stores before all its loads are issued, so memory-level
 // parallelism comes from the thread count, not from the warp count per row.
-// `lo` may be null: the mixed build's integration path fills the hi parts
-// only (the stencils never read the lo parts of ghosts), and fills the lo
-// parts on their own (as a block of floats) only when they are read.
+// The mixed build's integration path fills the hi parts only (the stencils
+// never read the lo parts of ghosts), and fills the lo block on its own (its
+// ACB_LO_NARR arrays of 8-byte elements) only when the lo parts are read.
 //
 // Sub-box fill (any start/end, any field range): one warp per (j, k) row of the
 // box, lane-strided; kept for the reference's partial-box API calls.
@@ -34,7 +34,7 @@
 struct HaloArgs {
     Layout L;
     state_t* block; // block (in)
-    float* lo;      // mixed build: lo block of `in` (else null)
+    lo16_t* lo;     // mixed build: lo block of `in` (bf16, see common.cuh; else null)
     int3 start, end;
     int f0, f1; // fields [f0, f1)
     long long rows;
@@ -49,7 +49,7 @@ wrap_interior(int c, int n)
 // Fills the ghost vertices of row (j, k) of the box [start, end) for fields
 // [f0, f1), with the 32 lanes of one warp.
 __device__ __forceinline__ void
-halo_row(const Layout& L, state_t* block, float* lo, int3 start, int3 end, int f0, int f1, int j,
+halo_row(const Layout& L, state_t* block, lo16_t* lo, int3 start, int3 end, int f0, int f1, int j,
          int k, int lane)
 {
     const bool ghost_row = j < NGHOST || j >= NGHOST + L.ny || k < NGHOST || k >= NGHOST + L.nz;
@@ -65,9 +65,9 @@ halo_row(const Layout& L, state_t* block, float* lo, int3 start, int3 end, int f
             for (int i = start.x + lane; i < end.x; i += 32)
                 F[(drow + i) * W] = F[(srow + wrap_interior(i, L.nx)) * W];
             if (ACB_MIXED && lo) {
-                float* G = lo + fidx(L, f, 0);
+                lo16_t* G = lo_field(lo, L, f);
                 for (int i = start.x + lane; i < end.x; i += 32)
-                    G[(drow + i) * W] = G[(srow + wrap_interior(i, L.nx)) * W];
+                    G[(drow + i) * ACB_LO_STEP] = G[(srow + wrap_interior(i, L.nx)) * ACB_LO_STEP];
             }
         }
     }
@@ -79,8 +79,8 @@ halo_row(const Layout& L, state_t* block, float* lo, int3 start, int3 end, int f
                 state_t* F         = block + fidx(L, f, 0);
                 F[(drow + i) * W] = F[(srow + is) * W];
                 if (ACB_MIXED && lo) {
-                    float* G         = lo + fidx(L, f, 0);
-                    G[(drow + i) * W] = G[(srow + is) * W];
+                    lo16_t* G                    = lo_field(lo, L, f);
+                    G[(drow + i) * ACB_LO_STEP] = G[(srow + is) * ACB_LO_STEP];
                 }
             }
         }
@@ -111,18 +111,19 @@ halo_chunks(const Layout& L)
     return (unsigned)(L.mx + 127) / 128;
 }
 
-// Work units of kind A (interior rows x arrays) and A + B of one mesh.
+// Work units of kind A (interior rows x arrays) and A + B of one block of
+// narr arrays (ACB_NARR for the fields, ACB_LO_NARR for the mixed lo block).
 static inline long long
-halo_units_a(const Layout& L)
+halo_units_a(const Layout& L, int narr = ACB_NARR)
 {
-    return (long long)L.ny * L.nz * ACB_NARR;
+    return (long long)L.ny * L.nz * narr;
 }
 
 static inline long long
-halo_units(const Layout& L)
+halo_units(const Layout& L, int narr = ACB_NARR)
 {
     const long long ghost_rows = (long long)L.my * L.mz - (long long)L.ny * L.nz;
-    return halo_units_a(L) + ghost_rows * ACB_NARR * halo_chunks(L) * 32;
+    return halo_units_a(L, narr) + ghost_rows * narr * halo_chunks(L) * 32;
 }
 
 // Periodic source of ghost-or-interior coordinate c in [0, n + 6), n >= NGHOST.
@@ -135,15 +136,15 @@ wrap_near(int c, int n)
 // The block's elements as 8-byte units (a field pair, or a double).
 typedef unsigned long long helem_t;
 
-// Kind A or B unit u of one block (hi parts, or the lo parts in the mixed
-// build: the same layout).
+// Kind A or B unit u of one block of narr arrays (the fields, or the mixed
+// build's lo block: the same geometry).
 __device__ __forceinline__ void
-halo_unit_block(const Layout& L, helem_t* block, unsigned units_a, unsigned u)
+halo_unit_block(const Layout& L, helem_t* block, unsigned units_a, unsigned u, unsigned narr)
 {
     if (u < units_a) {
         // kind A: x-ghosts of interior row r, array a
-        const unsigned ar    = u % ACB_NARR;
-        const unsigned r     = u / ACB_NARR;
+        const unsigned ar    = u % narr;
+        const unsigned r     = u / narr;
         const unsigned kq    = r / (unsigned)L.ny;
         const int j          = NGHOST + (int)(r - kq * (unsigned)L.ny);
         const int k          = NGHOST + (int)kq;
@@ -184,8 +185,8 @@ halo_unit_block(const Layout& L, helem_t* block, unsigned units_a, unsigned u)
     u -= units_a;
     const unsigned lane = u & 31;
     unsigned wq         = u >> 5;
-    const unsigned ar   = wq % ACB_NARR;
-    wq /= ACB_NARR;
+    const unsigned ar   = wq % narr;
+    wq /= narr;
     const unsigned nch   = halo_chunks(L);
     const unsigned row   = wq / nch;
     const unsigned chunk = wq - row * nch;
@@ -224,27 +225,27 @@ halo_unit_block(const Layout& L, helem_t* block, unsigned units_a, unsigned u)
     }
 }
 
+// the field block (ACB_NARR arrays) of a whole-box fill
 __device__ __forceinline__ void
-halo_unit(const Layout& L, void* block, void* lo, unsigned units_a, unsigned u)
+halo_unit(const Layout& L, void* block, unsigned units_a, unsigned u)
 {
-    halo_unit_block(L, static_cast<helem_t*>(block), units_a, u);
-    if (lo)
-        halo_unit_block(L, static_cast<helem_t*>(lo), units_a, u);
+    halo_unit_block(L, static_cast<helem_t*>(block), units_a, u, ACB_NARR);
 }
 
+// Whole-box fill of one block of narr arrays of 8-byte elements (the fields,
+// or the mixed build's lo block).
 static __global__ void __launch_bounds__(256)
-halo_full_kernel(const Layout L, state_t* block, float* lo, unsigned units_a, unsigned units)
+halo_full_kernel(const Layout L, void* block, unsigned units_a, unsigned units, unsigned narr)
 {
     const unsigned stride = gridDim.x * blockDim.x;
     for (unsigned u = blockIdx.x * blockDim.x + threadIdx.x; u < units; u += stride)
-        halo_unit(L, block, lo, units_a, u);
+        halo_unit_block(L, static_cast<helem_t*>(block), units_a, u, narr);
 }
 
 // One member of a batched ghost fill (whole m-box of every field).
 struct HaloMember {
     Layout L;
     state_t* block;
-    float* lo;
     long long unit_begin; // first global work unit of this member
     unsigned units_a;     // its kind-A units
 };
@@ -266,7 +267,7 @@ halo_batch_kernel(const HaloMember* __restrict__ mem, int n, long long total_uni
                 hi = mid - 1;
         }
         const HaloMember& m = mem[lo];
-        halo_unit(m.L, m.block, m.lo, m.units_a, (unsigned)(u - m.unit_begin));
+        halo_unit(m.L, m.block, m.units_a, (unsigned)(u - m.unit_begin));
     }
 }
 
@@ -309,8 +310,10 @@ mirror_kernel(const HaloArgs a, const float sign)
                 state_t* F        = a.block + fidx(L, f, 0);
                 F[(drow + i) * W] = (state_t)sign * F[(srow + is) * W];
                 if (ACB_MIXED && a.lo) {
-                    float* G          = a.lo + fidx(L, f, 0);
-                    G[(drow + i) * W] = sign * G[(srow + is) * W];
+                    // a bf16 value times -1 is its sign bit flipped
+                    lo16_t* G = lo_field(a.lo, L, f);
+                    const lo16_t v = G[(srow + is) * ACB_LO_STEP];
+                    G[(drow + i) * ACB_LO_STEP] = sign < 0 ? (lo16_t)(v ^ 0x8000u) : v;
                 }
             }
         }

@@ -107,9 +107,10 @@ AcResult prepare_table(const SolveConfig* cfgs, int n);
 // 4-D map (x, y, z, field) over a field block with a (TX+8, TY+6, 1, 8) box
 AcResult encode_block_map(const Layout& L, const state_t* block, const SolveConfig& cfg,
                           CUtensorMap* map);
-// the same with a (TX, TY, 1, 8) box: a tile's centre values (4-byte elements)
+// the same with a (TX, TY, 1, narr) box over a block of narr arrays: a tile's
+// centre values (the fields' narr = ACB_NARR, the mixed lo block's ACB_LO_NARR)
 AcResult encode_centre_map(const Layout& L, const void* block, const SolveConfig& cfg,
-                           CUtensorMap* map);
+                           CUtensorMap* map, int narr);
 
 // kernel arguments from a parameter mirror: coefficients pre-scaled in double
 // and rounded once to AcReal; rkA/rkB for `step` from AC_dt
@@ -139,7 +140,7 @@ void stage_destroy(StageBuf* stage);
 // between host memory (reference order) and the padded device layout through
 // the staging buffer; zeroes the lo parts of loaded values when given.
 AcResult copy_field_range(cudaStream_t st, const Layout& L, state_t* field, size_t s,
-                          AcReal* host, size_t count, bool h2d, float* lo_field,
+                          AcReal* host, size_t count, bool h2d, lo16_t* lo_field,
                           StageBuf* stage);
 
 } // namespace acb_host

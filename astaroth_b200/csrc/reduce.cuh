@@ -24,7 +24,7 @@ enum { RED_SCAL = 1, RED_VEC = 3, RED_ALFVEN = 4 };
 struct ReduceArgs {
     Layout L;
     const state_t* f[4];
-    const float* lo[4]; // mixed build: lo parts (else null)
+    const lo16_t* lo[4]; // mixed build: lo parts, lo_field views (else null)
     int nin;            // 1, 3 or 4
     int rtype;          // ReductionType
     int3 start, end;
@@ -61,7 +61,7 @@ red_load(const ReduceArgs& a, int w, long long id)
     // values further per element
     double v = (double)a.f[w][id * ACB_LANES];
 #if ACB_MIXED
-    v += (double)a.lo[w][id * ACB_LANES];
+    v += (double)lo16_to_float(a.lo[w][id * ACB_LO_STEP]);
 #endif
     return v;
 }

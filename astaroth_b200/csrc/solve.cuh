@@ -92,16 +92,16 @@ struct __align__(128) MemberDesc {
     SolveGeom g;
     long long task_begin; // first global task of this member (tasks are member-major)
     state_t* out;
-    float* in_lo;
-    float* out_lo;
+    lo16_t* in_lo;
+    lo16_t* out_lo;
 };
 
 template <typename T>
 struct SolveArgs {
     SolveGeom g;
     state_t* out;    // out block (previous state at s > 0; result)
-    float* in_lo;    // mixed build: lo parts of `in`
-    float* out_lo;   // mixed build: lo parts of `out`
+    lo16_t* in_lo;   // mixed build: lo block of `in` (bf16, see common.cuh)
+    lo16_t* out_lo;  // mixed build: lo block of `out`
     unsigned* status;
     SolveParams<T> P;
     // step diagnostics (kernels built with DIAG): four FP64 partials per CTA,
@@ -147,7 +147,7 @@ struct EnsSolveArgs : SolveArgs<T> {
 
 // Centre-only arrays of a substep that the ring does not carry: the previous
 // state (s > 0) and, in the mixed build, the lo parts of `in` and (s > 0) of
-// `out`. Map slots: 0 = out hi, 1 = in lo, 2 = out lo.
+// `out` (two lo arrays each, bf16). Map slots: 0 = out hi, 1 = in lo, 2 = out lo.
 template <int STEP>
 struct CentreSet {
     static constexpr bool PREV = STEP > 0;
@@ -159,10 +159,6 @@ struct CentreSet {
     // on memory (long-scoreboard stalls 1.66 per issued instruction at 256^3;
     // the 512^3 step 17.43 -> 17.22 ms, same-box A/B)
     static constexpr bool STAGE = N >= 1;
-    // position of each map's array in a centre slot (-1: not loaded)
-    static constexpr int POS_PREV    = PREV ? 0 : -1;
-    static constexpr int POS_CUR_LO  = LO ? (PREV ? 1 : 0) : -1;
-    static constexpr int POS_PREV_LO = (LO && PREV) ? 2 : -1;
 };
 
 struct CentreMaps {
@@ -176,6 +172,7 @@ struct TileCfg {
     // arrive by TMA in a ring of NC output-plane slots (else plain loads)
     static constexpr int NC = NC_;
     static constexpr int CENTRE = TX_ * TY_ * ACB_NARR; // elements of one centre array set
+    static constexpr int CENTRE_LO = TX_ * TY_ * ACB_LO_NARR; // the same for a lo block
     static constexpr int BX = TX_ + 8, BY = TY_ + 6;
     static constexpr int CONSUMERS = TX_ * TY_;        // one thread per (x, y) column
     static constexpr int CWARPS    = CONSUMERS / 32;   // consumer warps
@@ -195,9 +192,10 @@ struct TileCfg {
     static constexpr int FIELD   = BX * BY;           // elements per array of a ring slot
     static constexpr int PLANE   = ACB_NARR * FIELD;  // elements per ring slot
     static constexpr size_t ring_bytes() { return (size_t)NP * PLANE * ACB_ELEM; }
+    // prev hi, then (mixed) cur lo and prev lo
     static constexpr size_t centre_slot_bytes()
     {
-        return (size_t)(ACB_MIXED ? 3 : 1) * CENTRE * ACB_ELEM;
+        return (size_t)(ACB_MIXED ? CENTRE + 2 * CENTRE_LO : CENTRE) * ACB_ELEM;
     }
     static constexpr size_t smem_bytes() { return ring_bytes() + NC * centre_slot_bytes(); }
     // A task starts once the first 2 NGHOST planes are in the ring (the queue
@@ -884,6 +882,26 @@ load_centre(const Layout& L, const state_t* out, long long id, CentreVals& c)
             c.prev[f] = out[fidx(L, f, id)];
 }
 
+// The lo parts of pair array ar from a lo element (two bf16x2 words, the
+// even array's in the low one) as a float pair, and a float pair as a bf16x2
+// word (lane A in the low half); bf16 to float is exact.
+__device__ __forceinline__ acb::F2
+lo_unpack(unsigned long long e, int ar)
+{
+    const uint32_t x = (ar & 1) ? (uint32_t)(e >> 32) : (uint32_t)e;
+    return acb::pk2(__uint_as_float(x << 16), __uint_as_float(x & 0xffff0000u));
+}
+
+__device__ __forceinline__ uint32_t
+lo_pack(acb::F2 v)
+{
+    float a, b;
+    acb::upk2(v, a, b);
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a)); // b high, a low
+    return r;
+}
+
 // Single-precision layout: one (A, B) element per pair array; lo parts in
 // the mixed build.
 struct CentreVals2 {
@@ -894,22 +912,25 @@ struct CentreVals2 {
 
 template <int STEP>
 __device__ __forceinline__ void
-load_centre2(const Layout& L, const state_t* out, const float* in_lo, const float* out_lo,
+load_centre2(const Layout& L, const state_t* out, const lo16_t* in_lo, const lo16_t* out_lo,
              long long id, CentreVals2& c)
 {
-    const acb::F2* o  = reinterpret_cast<const acb::F2*>(out);
-    const acb::F2* il = reinterpret_cast<const acb::F2*>(in_lo);
-    const acb::F2* ol = reinterpret_cast<const acb::F2*>(out_lo);
+    const acb::F2* o               = reinterpret_cast<const acb::F2*>(out);
+    const unsigned long long* il   = reinterpret_cast<const unsigned long long*>(in_lo);
+    const unsigned long long* ol   = reinterpret_cast<const unsigned long long*>(out_lo);
 #pragma unroll
     for (int a = 0; a < ACB_NARR; ++a) {
         const long long e = a * L.fstride + id;
         if (STEP > 0)
             c.prev[a] = o[e];
 #if ACB_MIXED
-        c.cur_lo[a]  = il[e];
-        c.prev_lo[a] = STEP > 0 ? ol[e] : acb::F2{0ull};
+        const long long el = (a >> 1) * L.fstride + id;
+        c.cur_lo[a]        = lo_unpack(il[el], a);
+        c.prev_lo[a]       = STEP > 0 ? lo_unpack(ol[el], a) : acb::F2{0ull};
 #endif
     }
+    (void)il;
+    (void)ol;
 }
 
 template <class Cfg>
@@ -959,7 +980,7 @@ member_of(const MemberDesc<T>* md, int n, long long t)
 template <class Cfg, int STEP, bool ENS, bool DTDEV, bool DIAG, class PT>
 __device__ __forceinline__ bool
 consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
-             long long lt, state_t* out, float* in_lo, float* out_lo, const void* ring,
+             long long lt, state_t* out, lo16_t* in_lo, lo16_t* out_lo, const void* ring,
              uint64_t* full, uint64_t* empty, volatile int* abort_flag, uint32_t& q,
              const void* centre, uint64_t* full_c, uint64_t* empty_c, uint32_t& oq,
              DiagAcc& dacc)
@@ -1068,22 +1089,29 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
                     acb::forcing_at<T>(a.P, i, j, k, fo);
                 if constexpr (CT) {
                     // from the centre slot the producer filled by TMA
+                    // slot: prev hi [array][TY][TX], then cur lo and prev lo
+                    // [lo array][TY][TX], 8-byte elements
                     const acb::F2* cs = reinterpret_cast<const acb::F2*>(centre) +
                                         (size_t)(oq % Cfg::NC) * (Cfg::centre_slot_bytes() / 8) +
                                         ty * TX + tx;
-                    constexpr int FS = Cfg::TX * Cfg::TY;
+                    const unsigned long long* csu =
+                        reinterpret_cast<const unsigned long long*>(cs);
+                    constexpr int FS  = Cfg::TX * Cfg::TY;
+                    constexpr int OCL = CS::PREV ? Cfg::CENTRE : 0; // cur lo
+                    constexpr int OPL = OCL + Cfg::CENTRE_LO;       // prev lo
 #pragma unroll
                     for (int ar = 0; ar < ACB_NARR; ++ar) {
                         if constexpr (CS::PREV)
-                            cv.prev[ar] = cs[CS::POS_PREV * Cfg::CENTRE + ar * FS];
+                            cv.prev[ar] = cs[ar * FS];
 #if ACB_MIXED
-                        cv.cur_lo[ar] = cs[CS::POS_CUR_LO * Cfg::CENTRE + ar * FS];
+                        cv.cur_lo[ar] = lo_unpack(csu[OCL + (ar >> 1) * FS], ar);
                         if constexpr (CS::PREV)
-                            cv.prev_lo[ar] = cs[CS::POS_PREV_LO * Cfg::CENTRE + ar * FS];
+                            cv.prev_lo[ar] = lo_unpack(csu[OPL + (ar >> 1) * FS], ar);
                         else
                             cv.prev_lo[ar] = acb::F2{0ull};
 #endif
                     }
+                    (void)csu;
                 }
                 // The update, two fields per instruction (one pair array):
                 //   FP32:  out = cur + rkA (cur - prev) + rkB roc  [+ forcing]
@@ -1095,7 +1123,8 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
                 const acb::F2 rkA2 = acb::pk2(rkA, rkA), rkB2 = acb::pk2(rkB, rkB);
                 acb::F2* o2 = reinterpret_cast<acb::F2*>(out);
 #if ACB_MIXED
-                acb::F2* ol2 = reinterpret_cast<acb::F2*>(out_lo);
+                unsigned long long* ol2 = reinterpret_cast<unsigned long long*>(out_lo);
+                uint32_t lo_even = 0; // the even array's bf16x2 word, stored with the odd one's
 #endif
                 // lane 0 of arrays 0..3 holds lnrho, ux, uy, uz: their stored
                 // values for the step diagnostics (hi and, mixed, lo)
@@ -1117,12 +1146,17 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
                     acb::pair_add2(cur2[ar], l2, d2, h2, w2);
                     if (STEP == 3 && ar >= 1)
                         acb::pair_add2(h2, w2, acb::pk2(fo[ar - 1], 0.f), h2, w2);
-                    o2[e]  = h2;
-                    ol2[e] = w2;
+                    o2[e] = h2;
+                    const uint32_t wl = lo_pack(w2); // lo rounded to bf16 as stored
+                    if (ar & 1)
+                        ol2[(ar >> 1) * L.fstride + id] =
+                            (unsigned long long)lo_even | ((unsigned long long)wl << 32);
+                    else
+                        lo_even = wl;
                     if constexpr (DIAG) {
                         float t_;
                         acb::upk2(h2, dh[ar], t_);
-                        acb::upk2(w2, dl[ar], t_);
+                        acb::upk2(lo_unpack(wl, 0), dl[ar], t_);
                     }
 #else
                     acb::F2 r;
@@ -1400,20 +1434,22 @@ __global__ void __launch_bounds__(Cfg::THREADS, Cfg::MINB)
                                 ok = false;
                                 break;
                             }
-                            constexpr uint32_t CB = Cfg::CENTRE * ACB_ELEM;
+                            constexpr uint32_t CB = Cfg::CENTRE * ACB_ELEM;    // prev hi
+                            constexpr uint32_t CL = Cfg::CENTRE_LO * ACB_ELEM; // a lo set
+                            constexpr uint32_t OC = CS::PREV ? CB : 0;        // cur lo
+                            constexpr uint32_t OP = OC + CL;                   // prev lo
+                            constexpr uint32_t TXB = (CS::PREV ? CB : 0) + (CS::LO ? CL : 0) +
+                                                     ((CS::LO && CS::PREV) ? CL : 0);
                             unsigned char* dst = centre + (size_t)sc * Cfg::centre_slot_bytes();
                             const int xc = g->L.offx + tg.i0; // interior tile start: 32-byte aligned
                             const int zc = tg.k0 + (l - 2 * NGHOST);
-                            mbar_arrive_expect_tx(&full_c[sc], CS::N * CB);
+                            mbar_arrive_expect_tx(&full_c[sc], TXB);
                             if (CS::PREV)
-                                tma_load_4d(dst + CS::POS_PREV * CB, &cm.m[0], xc, tg.j0, zc, 0,
-                                            &full_c[sc]);
+                                tma_load_4d(dst, &cm.m[0], xc, tg.j0, zc, 0, &full_c[sc]);
                             if (CS::LO)
-                                tma_load_4d(dst + CS::POS_CUR_LO * CB, &cm.m[1], xc, tg.j0, zc, 0,
-                                            &full_c[sc]);
+                                tma_load_4d(dst + OC, &cm.m[1], xc, tg.j0, zc, 0, &full_c[sc]);
                             if (CS::LO && CS::PREV)
-                                tma_load_4d(dst + CS::POS_PREV_LO * CB, &cm.m[2], xc, tg.j0, zc,
-                                            0, &full_c[sc]);
+                                tma_load_4d(dst + OP, &cm.m[2], xc, tg.j0, zc, 0, &full_c[sc]);
                             ++oq;
                         }
                     }

@@ -6,7 +6,8 @@ Workload (the headline configuration): 512^3 mesh, eight fields
 k = 2 velocity mode u = 0.1 (sin 2y, sin 2z, sin 2x), dx = 2 pi / 512,
 nu = eta = 5e-3, cs = 1, gamma = 5/3, cp = 1, dt = 1e-3, periodic.
 The measured arm is the mixed-precision library (FP32 stencils and right-hand
-sides, compensated (hi, lo) FP32 state, FP64 reductions); the plain FP64 and
+sides, compensated state: FP32 hi part and bfloat16 lo part, FP64 reductions);
+the plain FP64 and
 FP32 libraries run the same steps beside it for the comparison and the error.
 
 One step = three substeps, each a periodic ghost fill of all fields plus one
@@ -225,9 +226,9 @@ def host_mesh(flavour: str, n: int, pinned: bool = True, velocity_mode: float = 
 def alg_bytes_per_step(flavour: str, n: int) -> int:
     """Algorithmic HBM bytes of the three solve launches of one step: every
     array touched once per substep (s = 0: read in, write out; s = 1, 2: read
-    in, read out, write out), eight fields. FP32 4 B, FP64 8 B, mixed 8 B
-    (float hi + float lo) per value."""
-    w = {"sp": 4, "dp": 8, "mixed": 8}[flavour]
+    in, read out, write out), eight fields. FP32 4 B, FP64 8 B, mixed 6 B
+    (float hi + bfloat16 lo) per value: 256, 512 and 384 B per cell and step."""
+    w = {"sp": 4, "dp": 8, "mixed": 6}[flavour]
     return 8 * w * (2 + 3 + 3) * n ** 3
 
 
@@ -870,8 +871,9 @@ def measured_peak_hbm():
 
 
 def config_block(n: int, world: int) -> dict:
-    return {"workload": f"MHD RK3, {n}^3, 8 fields, mixed precision (FP32 RHS, compensated FP32 "
-                        f"state, FP64 reductions); seeded 1e-3 noise + k=2 velocity mode 0.1",
+    return {"workload": f"MHD RK3, {n}^3, 8 fields, mixed precision (FP32 RHS, compensated state "
+                        f"FP32 hi + bf16 lo, FP64 reductions); seeded 1e-3 noise + k=2 velocity "
+                        f"mode 0.1",
             "mesh": [n, n, n], "fields": 8, "dt": DT, "dx": "2*pi/n", "nu": 5e-3, "eta": 5e-3,
             "cs": 1.0, "gamma": 5.0 / 3.0, "cp": 1.0,
             "step": "3 x (periodic ghost fill + fused solve launch + swap) through the C ABI",
@@ -1006,7 +1008,8 @@ def run_ours(args) -> None:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32 (compensated f32-pair state, f64 reductions)", "data": "synthetic",
+                "dtype": "f32 (compensated state: f32 hi + bf16 lo, f64 reductions)",
+                "data": "synthetic",
                 "config": config_block(n, ranks.world),
                 "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak,
                              "unit": "GB/s", "frac": achieved_gbs / peak,
