@@ -250,18 +250,29 @@ struct HaloMember {
     unsigned units_a;     // its kind-A units
 };
 
+// Members whose first work units a fill block keeps in shared memory.
+constexpr int ACB_HALO_SEARCH = 1024;
+
 // Ghost fill of every field of many meshes in one launch; threads take the
-// concatenated work units of all members.
+// concatenated work units of all members. A unit's member is found by binary
+// search over the members' first units, held in shared memory (the first
+// ACB_HALO_SEARCH members; any further ones are read from the table), so the
+// search costs shared loads instead of a chain of dependent global ones.
 static __global__ void __launch_bounds__(256)
 halo_batch_kernel(const HaloMember* __restrict__ mem, int n, long long total_units)
 {
+    __shared__ long long first[ACB_HALO_SEARCH];
+    const int ns = n < ACB_HALO_SEARCH ? n : ACB_HALO_SEARCH;
+    for (int i = threadIdx.x; i < ns; i += blockDim.x)
+        first[i] = mem[i].unit_begin;
+    __syncthreads();
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < total_units;
          u += stride) {
         int lo = 0, hi = n - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (mem[mid].unit_begin <= u)
+            if ((mid < ns ? first[mid] : mem[mid].unit_begin) <= u)
                 lo = mid;
             else
                 hi = mid - 1;
