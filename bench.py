@@ -295,7 +295,10 @@ def e2e_run(flavour: str, host, steps: int, ranks) -> dict:
     """The same steps end to end through the public C ABI with host buffers:
     load the mesh from pinned host memory, per step one RK3 step
     (acDeviceIntegrateStep) and one diagnostic reduction read back to the host
-    (max |u|, as a CFL check does), then store the mesh to pinned host memory."""
+    (max |u|, as a CFL check does), then store the mesh to pinned host memory.
+    The reduction is folded into each step's last substep
+    (acDeviceSetStepDiagnostics), so acDeviceReduceVec(MAX) returns it with one
+    small device-to-host copy instead of another pass over the fields."""
     import torch
 
     from astaroth_b200 import Device, abi
@@ -303,6 +306,7 @@ def e2e_run(flavour: str, host, steps: int, ranks) -> dict:
     n = abi.dims(host.info)[0]
     dev = Device(flavour, host.info, torch.cuda.current_device())
     out = abi.HostMesh(host.prec, host.info, pinned=True)
+    dev.set_step_diagnostics(True)
     dev.load_mesh(host)
     dev.integrate_step(DT)  # warm the kernels and graph-free path
     dev.synchronize()
@@ -320,7 +324,7 @@ def e2e_run(flavour: str, host, steps: int, ranks) -> dict:
     dev.destroy()
     del out
     return {"seconds": t, "cells_per_s": ranks.world * n ** 3 * steps / t,
-            "h2d_bytes_per_step": mesh_bytes / steps, "d2h_bytes_per_step": 8 + mesh_bytes / steps,
+            "h2d_bytes_per_step": mesh_bytes / steps, "d2h_bytes_per_step": 32 + mesh_bytes / steps,
             "umax": umax}
 
 
@@ -845,20 +849,24 @@ def cfl_run(sizes, steps: int, warmup: int, ranks, gpu: int) -> dict:
     return out
 
 
-def profile_traffic(name: str):
-    """Per-launch DRAM bytes of the dominant kernel from a committed ncu
-    summary (a line `traffic_bytes_per_launch: <value>`), else None."""
+def profile_traffic(name: str, n: int):
+    """DRAM bytes per solve launch of an n^3 step from a committed ncu capture
+    (profiles/<name>, JSON): the mean over the step's three launches (s = 2 as
+    recorded in the file) of dram__bytes_read.sum + dram__bytes_write.sum,
+    scaled from the captured mesh by the cells (a launch's bytes grow with the
+    cells it updates); None when the file is absent."""
     path = os.path.join(HERE, "profiles", name)
-    if not os.path.exists(path):
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        launches = p["launches"]
+        per = []
+        for s in ("s0", "s1", "s2"):
+            rec = launches.get(s) or launches[p[s + "_as"]]
+            per.append(rec["dram_bytes_read"] + rec["dram_bytes_write"])
+        return sum(per) / len(per) * n ** 3 / p["cells"]
+    except (OSError, KeyError, ValueError, TypeError):
         return None
-    with open(path) as f:
-        for line in f:
-            if line.strip().startswith("traffic_bytes_per_launch:"):
-                try:
-                    return float(line.split(":", 1)[1].split()[0])
-                except ValueError:
-                    return None
-    return None
 
 
 def measured_peak_hbm():
@@ -928,9 +936,10 @@ def run_ours(args) -> None:
     alg = alg_bytes_per_step(arm, n)
     achieved_gbs = alg * args.steps / (res["solve_ms_total"] * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    # DRAM bytes of one s = 1 launch at this size, from the committed ncu
-    # summary of a 256^3 capture scaled by the cells (bytes grow with them)
-    traffic = profile_traffic("solve_mixed_256.md")
+    # DRAM bytes per solve launch at this size (mean over the step's three
+    # launches), from the committed ncu capture of a 256^3 step scaled by the
+    # cells (bytes grow with them)
+    traffic = profile_traffic(f"solve_{arm}_256.json", n)
 
     variants = {}
     errors = None
@@ -975,7 +984,8 @@ def run_ours(args) -> None:
         e2e = {"value": e["cells_per_s"], "unit": UNIT,
                "h2d_bytes_per_step": e["h2d_bytes_per_step"],
                "d2h_bytes_per_step": e["d2h_bytes_per_step"],
-               "includes": "mesh load from pinned host, per-step max|u| read back, mesh store"}
+               "includes": "mesh load from pinned host, per-step max|u| (folded into the step's "
+                           "last substep) read back, mesh store"}
         del h
 
     ensemble = None
@@ -1008,7 +1018,8 @@ def run_ours(args) -> None:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32 (compensated state: f32 hi + bf16 lo, f64 reductions)",
+                "dtype": {"mixed": "f32 (compensated state: f32 hi + bf16 lo, f64 reductions)",
+                          "sp": "f32", "dp": "f64"}[arm],
                 "data": "synthetic",
                 "config": config_block(n, ranks.world),
                 "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak,
