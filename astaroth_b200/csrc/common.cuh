@@ -3,8 +3,9 @@
 // One source tree is compiled three times (see astaroth_b200/build.py):
 //   sp     AC_DOUBLE_PRECISION=0                   float state, FP32 kernels
 //   dp     AC_DOUBLE_PRECISION=1                   double state, FP64 kernels
-//   mixed  AC_DOUBLE_PRECISION=0 ACB_MIXED=1       float interface; (hi, lo)
-//          float state, FP32 stencils/RHS, compensated RK3 update, FP64 sums
+//   mixed  AC_DOUBLE_PRECISION=0 ACB_MIXED=1       float interface; state of a
+//          float hi and a bfloat16 lo part, FP32 stencils/RHS, compensated RK3
+//          update, FP64 sums
 #pragma once
 
 #include <cuda.h>

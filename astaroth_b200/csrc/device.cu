@@ -526,8 +526,9 @@ launch_solve(const Device d, cudaStream_t st, int step, int3 s, int3 e,
 }
 
 // Fills the lo parts of block b's ghosts with their periodic images if the last
-// whole-box fill of b left them (see lo_stale): the lo block is a block of
-// floats with the same layout, filled like the hi parts.
+// whole-box fill of b left them (see lo_stale): the lo block has the layout of
+// the hi block with ACB_LO_NARR arrays of 8-byte elements (four bfloat16 lo
+// parts each), filled like the hi parts.
 static AcResult
 ensure_lo_ghosts(const Device d, cudaStream_t st, int b)
 {
@@ -1046,7 +1047,7 @@ acDevicePrintInfo(const Device device)
     printf("    Shared memory per block (opt-in): %zu KiB\n", p.sharedMemPerBlockOptin / 1024);
     printf("  Mesh %d x %d x %d, row pitch %d, %s state\n", device->L.nx, device->L.ny,
            device->L.nz, device->L.mxp,
-           ACB_MIXED ? "mixed (hi, lo) float" : (sizeof(AcReal) == 8 ? "double" : "float"));
+           ACB_MIXED ? "mixed (float hi, bfloat16 lo)" : (sizeof(AcReal) == 8 ? "double" : "float"));
     printf("  Solve configuration: %s\n", cfgs[device->solve_cfg].name);
     printf("--------------------------------------------------\n");
     return AC_SUCCESS;

@@ -38,8 +38,9 @@
 //   - derivative coefficients arrive pre-scaled by 1/ds (and 1/ds^2) so each
 //     pencil costs 6-7 FP ops; only the 21 first, 24 second and 12 cross
 //     derivatives the right-hand sides use are formed;
-//   - the mixed build keeps the state as an unevaluated float pair (hi, lo):
-//     stencils read hi, the update is a compensated two-sum.
+//   - the mixed build keeps the state as an unevaluated sum hi + lo of a float
+//     and a bfloat16 (stored as such, widened to float in registers): stencils
+//     read hi, the update is a compensated two-sum.
 #pragma once
 #include <type_traits>
 

@@ -15,8 +15,8 @@
  *   libastaroth_sp.so     AcReal = float,  FP32 kernels
  *   libastaroth_dp.so     AcReal = double, FP64 kernels
  *   libastaroth_mixed.so  AcReal = float at the interface; FP32 stencils and
- *                         right-hand sides with a compensated (hi, lo) FP32
- *                         state and FP64 reductions inside.
+ *                         right-hand sides with a compensated state (a float hi
+ *                         and a bfloat16 lo part) and FP64 reductions inside.
  */
 #pragma once
 #include <cuda_runtime_api.h> /* int3, float3, double3 */

@@ -189,8 +189,9 @@ AcResult acEnsembleAutoOptimize(Ensemble ensemble, const char* cache_path);
 
 /* Loads / stores one whole field (mx*my*mz values, reference index order)
  * from / to a double array. In the mixed build the double is split into the
- * (hi, lo) float pair on load and recombined on store, so the state round
- * trips at ~48-bit precision. */
+ * state's float hi part and bfloat16 lo part on load and recombined on store,
+ * so a value round trips to about 32 significant bits (24 in hi, 8 more in lo;
+ * relative error below 2^-32). */
 AcResult acDeviceLoadVertexBufferDouble(const Device device, const Stream stream,
                                         const VertexBufferHandle handle, const double* src);
 AcResult acDeviceStoreVertexBufferDouble(const Device device, const Stream stream,
