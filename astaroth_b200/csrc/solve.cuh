@@ -934,6 +934,35 @@ load_centre2(const Layout& L, const state_t* out, const lo16_t* in_lo, const lo1
     (void)ol;
 }
 
+// The same values of the vertex a plane above into L1, while this plane's
+// right-hand sides run (their plain loads then hit L1 instead of waiting on
+// memory: FP32 512^3 step 13.17 -> 13.07 ms, FP32 ensemble step 5.52 -> 5.41 ms).
+template <int STEP>
+__device__ __forceinline__ void
+prefetch_centre2(const Layout& L, const state_t* out, const lo16_t* in_lo, const lo16_t* out_lo,
+                 long long id)
+{
+    const acb::F2* o             = reinterpret_cast<const acb::F2*>(out);
+    const unsigned long long* il = reinterpret_cast<const unsigned long long*>(in_lo);
+    const unsigned long long* ol = reinterpret_cast<const unsigned long long*>(out_lo);
+#pragma unroll
+    for (int a = 0; a < ACB_NARR; ++a) {
+        if (STEP > 0)
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(o + a * L.fstride + id));
+#if ACB_MIXED
+        if ((a & 1) == 0) {
+            const long long el = (a >> 1) * L.fstride + id;
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(il + el));
+            if (STEP > 0)
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(ol + el));
+        }
+#endif
+    }
+    (void)o;
+    (void)il;
+    (void)ol;
+}
+
 template <class Cfg>
 struct TaskGeom {
     int i0, j0, k0, nout;
@@ -1080,8 +1109,11 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
                 // first, or (CT) read from the centre slot after the right-hand
                 // sides, which keeps their registers free through the stencils
                 CentreVals2 cv;
-                if constexpr (!CT)
+                if constexpr (!CT) {
                     load_centre2<STEP>(L, out, in_lo, out_lo, id, cv);
+                    if (p + 1 < tg.nout)
+                        prefetch_centre2<STEP>(L, out, in_lo, out_lo, id + L.plane);
+                }
                 const acb::F2* c = reinterpret_cast<const acb::F2*>(ring) + (size_t)sc * PLANE + col;
                 float roc[ACB_NF], cur[ACB_NF];
                 acb::F2 cur2[ACB_NARR];
