@@ -66,8 +66,8 @@ struct SolveParams {
     // built with DTDEV take rkB = (T)(rk_beta * *dt_dev) instead of rkB above
     const double* dt_dev;
     double rk_beta;
-    // 2 pi / (ds n) per axis in double precision: the mixed build forms the
-    // forcing phase in double (forcing_at)
+    // 2 pi / (ds n) per axis in double precision: the single-precision builds
+    // form the forcing phase in double (forcing_column, forcing_plane)
     double fxs_d[3];
 };
 
@@ -777,26 +777,14 @@ rhs_terms(const FieldDerivs<T>& lr, const FieldDerivs<T>& ux, const FieldDerivs<
 }
 
 // Helical forcing at interior vertex (i, j, k) (stencil_kernel.ac:611-648 with
-// a single device: global index = local index, global grid = local grid).
+// a single device: global index = local index, global grid = local grid), the
+// double-precision build's; the single-precision builds form the phase by
+// parts (forcing_column, forcing_plane and forcing_from below).
 template <typename T>
 __device__ __forceinline__ void
 forcing_at(const SolveParams<T>& P, int i, int j, int k, T f[3])
 {
     T skx, ckx;
-#if ACB_MIXED
-    // mixed build: the phase k.x in double precision, reduced to [-pi, pi]
-    // before the single-precision sincos, so the forcing carries the error of
-    // its own size rather than that of a phase of up to |k| 2 pi (in single
-    // precision its ulp, ~4e-6 at a phase of 30, passes into the velocity)
-    {
-        const double x0  = ((double)(i - NGHOST) * (double)P.fds[0]) * P.fxs_d[0];
-        const double x1  = ((double)(j - NGHOST) * (double)P.fds[1]) * P.fxs_d[1];
-        const double x2  = ((double)(k - NGHOST) * (double)P.fds[2]) * P.fxs_d[2];
-        const double kxd = (double)P.fk[0] * x0 + (double)P.fk[1] * x1 + (double)P.fk[2] * x2;
-        const double red = kxd - 6.283185307179586 * rint(kxd * 0.15915494309189535);
-        sincosf((float)red, (float*)&skx, (float*)&ckx);
-    }
-#else
     const T x0 = (T)(i - NGHOST) * P.fds[0] * P.fxs[0];
     const T x1 = (T)(j - NGHOST) * P.fds[1] * P.fxs[1];
     const T x2 = (T)(k - NGHOST) * P.fds[2] * P.fxs[2];
@@ -807,13 +795,67 @@ forcing_at(const SolveParams<T>& P, int i, int j, int k, T f[3])
     else {
         sincos((double)kx, (double*)&skx, (double*)&ckx);
     }
-#endif
     const T re = ckx * P.fcphi - skx * P.fsphi;
     const T im = ckx * P.fsphi + skx * P.fcphi;
     bool ok    = true;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         f[c] = P.fscale * (P.ff_re[c] * re - P.ff_im[c] * im);
+        ok   = ok && isfinite(f[c]);
+    }
+    if (!ok)
+        f[0] = f[1] = f[2] = 0;
+}
+
+// sin and cos of a double-precision phase, reduced to [-pi, pi] in double
+// precision first
+__device__ __forceinline__ void
+sincos_reduced(double ph, float& s, float& c)
+{
+    const double red = ph - 6.283185307179586 * rint(ph * 0.15915494309189535);
+    sincosf((float)red, &s, &c);
+}
+
+// The single-precision builds' forcing, by parts: the phase k.x + phi of
+// vertex (i, j, k) is (k_x x + k_y y) + k_z z + phi, and exp(i (k.x + phi)) is
+// the product of exp(i (k_x x + k_y y + phi)), formed once per column of a task
+// (forcing_column), and exp(i k_z z), once per plane (forcing_plane; a warp's
+// lanes form 32 planes' at a time, shuffled to the vertex's plane). Each part's
+// phase is formed in double precision and reduced before its sin and cos, as
+// forcing_at does for the whole phase; the product adds one rounding of a unit
+// complex number. The exponentials then cost once per column and plane instead
+// of once per vertex (the forced substep 2: 5.79 -> 5.44 ms at 512^3, 49.4 ->
+// 46.3 ms at 1024^3, same-box A/B).
+template <typename T>
+__device__ __forceinline__ void
+forcing_column(const SolveParams<T>& P, int i, int j, float& cxy, float& sxy)
+{
+    const double x0 = ((double)(i - NGHOST) * (double)P.fds[0]) * P.fxs_d[0];
+    const double x1 = ((double)(j - NGHOST) * (double)P.fds[1]) * P.fxs_d[1];
+    float s, c;
+    sincos_reduced((double)P.fk[0] * x0 + (double)P.fk[1] * x1, s, c);
+    cxy = c * (float)P.fcphi - s * (float)P.fsphi; // times exp(i phi)
+    sxy = s * (float)P.fcphi + c * (float)P.fsphi;
+}
+
+template <typename T>
+__device__ __forceinline__ void
+forcing_plane(const SolveParams<T>& P, int k, float& cz, float& sz)
+{
+    const double x2 = ((double)(k - NGHOST) * (double)P.fds[2]) * P.fxs_d[2];
+    sincos_reduced((double)P.fk[2] * x2, sz, cz);
+}
+
+template <typename T>
+__device__ __forceinline__ void
+forcing_from(const SolveParams<T>& P, float cxy, float sxy, float cz, float sz, T f[3])
+{
+    const float re = cxy * cz - sxy * sz;
+    const float im = sxy * cz + cxy * sz;
+    bool ok        = true;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        f[c] = (T)(P.fscale * (P.ff_re[c] * re - P.ff_im[c] * im));
         ok   = ok && isfinite(f[c]);
     }
     if (!ok)
@@ -1064,6 +1106,13 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
                 mbar_arrive(&empty[(q + l) % NP]);
     }
 
+    // forcing (s = 2 with forcing; single precision): the column's phase factor
+    float fcxy = 0.f, fsxy = 0.f, fcz = 0.f, fsz = 0.f;
+    if constexpr (STEP == 3 && QZ)
+        acb::forcing_column(a.P, i, j, fcxy, fsxy);
+    (void)fcxy;
+    (void)fsxy;
+
     // double precision (no queues, registers to spare for it): the centre
     // values of the next plane are loaded a plane ahead
     constexpr bool PREF = !QZ;
@@ -1092,6 +1141,15 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
             return false;
         }
         const int k = tg.k0 + p;
+        float fcb = 0.f, fsb = 0.f; // the plane's forcing phase factor
+        if constexpr (STEP == 3 && QZ) {
+            if ((p & 31) == 0) // lane l: plane p + l
+                acb::forcing_plane(a.P, k + lane, fcz, fsz);
+            fcb = __shfl_sync(0xffffffffu, fcz, p & 31);
+            fsb = __shfl_sync(0xffffffffu, fsz, p & 31);
+        }
+        (void)fcb;
+        (void)fsb;
         if (act) {
             const long long id = lidx(L, i, j, k);
             const uint32_t sc  = (q + p + NGHOST) % NP;
@@ -1119,7 +1177,7 @@ consume_task(const SolveArgs<AcReal>& a, const SolveGeom& gv, const PT& P,
                 acb::F2 cur2[ACB_NARR];
                 acb::mhd_rhs_q<BX, FIELD>(c, zo, P, roc, cur, cur2, Q);
                 if constexpr (STEP == 3)
-                    acb::forcing_at<T>(a.P, i, j, k, fo);
+                    acb::forcing_from<T>(a.P, fcxy, fsxy, fcb, fsb, fo);
                 if constexpr (CT) {
                     // from the centre slot the producer filled by TMA
                     // slot: prev hi [array][TY][TX], then cur lo and prev lo

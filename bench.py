@@ -554,7 +554,7 @@ def ensemble_run(steps: int, ranks) -> dict:
 
 def forced_run(n: int, steps: int, warmup: int, ranks, gpu: int) -> dict:
     """The forced large-mesh workload: an n^3 mixed-precision mesh (1024^3:
-    141 GB of (hi, lo) state in two buffers), the seeded initial state of the
+    105 GB of state, float hi and bfloat16 lo parts in two buffers), the seeded initial state of the
     headline workload, and every step a new helical forcing (|k| in [1, 3],
     magnitude 0.05, relhel 0, from the seeded generator acForcingParamsGenerate,
     seed 5) then one RK3 step then the diagnostics: max, min and rms of |u|
