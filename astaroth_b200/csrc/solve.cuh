@@ -784,17 +784,13 @@ template <typename T>
 __device__ __forceinline__ void
 forcing_at(const SolveParams<T>& P, int i, int j, int k, T f[3])
 {
+    static_assert(sizeof(T) == 8, "the single-precision builds use forcing_from");
     T skx, ckx;
     const T x0 = (T)(i - NGHOST) * P.fds[0] * P.fxs[0];
     const T x1 = (T)(j - NGHOST) * P.fds[1] * P.fxs[1];
     const T x2 = (T)(k - NGHOST) * P.fds[2] * P.fxs[2];
     const T kx = P.fk[0] * x0 + P.fk[1] * x1 + P.fk[2] * x2;
-    if constexpr (sizeof(T) == 4) {
-        sincosf((float)kx, (float*)&skx, (float*)&ckx);
-    }
-    else {
-        sincos((double)kx, (double*)&skx, (double*)&ckx);
-    }
+    sincos(kx, &skx, &ckx);
     const T re = ckx * P.fcphi - skx * P.fsphi;
     const T im = ckx * P.fsphi + skx * P.fcphi;
     bool ok    = true;
