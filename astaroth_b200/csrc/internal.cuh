@@ -20,11 +20,12 @@ using SolveCfg0 = TileCfg<32, 12, 6, 1, 2>;
 using SolveCfg1 = TileCfg<64, 4, 6, 1, 3>;
 using SolveCfg2 = TileCfg<32, 8, 7, 1, 3>;
 #else
-// the first (the default, 12 consumer warps) is the fastest at 512^3; 32-wide
-// tiles waste fewer columns on meshes whose nx is an odd multiple of 32
-using SolveCfg0 = TileCfg<64, 6, 7, 1>;
+// the first (the default, 12 consumer warps) is the fastest at 512^3 (12.53
+// against 12.63 ms per step for 64 x 6 tiles, same-box A/B); 32-wide tiles also
+// waste fewer columns on meshes whose nx is an odd multiple of 32
+using SolveCfg0 = TileCfg<32, 12, 7, 1>;
 using SolveCfg1 = TileCfg<32, 8, 9, 1>;
-using SolveCfg2 = TileCfg<32, 12, 7, 1>;
+using SolveCfg2 = TileCfg<64, 6, 7, 1>;
 #endif
 
 typedef void (*SolveKernelFn)(const CUtensorMap, const SolveArgs<AcReal>, const CentreMaps);
