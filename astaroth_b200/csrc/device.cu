@@ -90,24 +90,30 @@ struct device_s {
     CentreMaps cmap[2]; // by parity of `in`: centre boxes over out hi, in lo, out lo
     int tmap_cfg;       // configuration the maps were encoded for (-1: none)
 
-    double* red_partials; // 3 * red_max_blocks (the three-in-one pass)
+    double* red_partials; // 3 * ACB_RED_SETS * red_max_blocks (the multi-set pass)
     int red_max_blocks;
     unsigned* red_counter;
-    double* red_result; // 3 doubles
-    double* h_result;   // pinned, 3 doubles
+    double* red_result; // 3 * ACB_RED_SETS doubles
+    double* h_result;   // pinned, 3 * ACB_RED_SETS doubles
     // Interiors written so far: bumped by every operation that can change a
     // block's interior values (the solve, loads, fills of whole fields,
     // transfers, graph replays). A MAX / MIN / RMS reduction of one field or
-    // one vector's length computes all three in one pass (reduce3_kernel) and
-    // keeps them here with the block and the epoch they were taken at; the
-    // other two then come from this record while nothing has changed.
+    // one vector's length computes all three in one pass, together with those
+    // of the scalar fields whose bytes the pass reads anyway (a vector's
+    // components and, in the single-precision builds, the fields sharing
+    // their 8-byte elements), and keeps them here with the block and the epoch
+    // they were taken at; later requests for any of them come from this record
+    // while nothing has changed.
     unsigned long long write_epoch;
     struct {
         bool valid;
         const void* block;
         unsigned long long epoch;
-        int nin, handles[3];
-        double vals[3]; // MAX, MIN, RMS sum
+        int n; // entries, of every pass taken on this block and epoch
+        struct {
+            int nin, handles[3];
+            double vals[3]; // MAX, MIN, RMS sum
+        } e[ACB_RED_RECORD];
     } red3;
 
     // Step diagnostics folded by the last substep's solve launch (enabled by
@@ -653,30 +659,73 @@ run_reduce(const Device d, cudaStream_t st, int rtype, int nin, const int* handl
         return AC_SUCCESS;
     }
     if (which >= 0 && (nin == RED_SCAL || nin == RED_VEC)) {
-        // MAX, MIN and RMS together: one pass over the fields serves all three
-        // requests while the block is unchanged (the diagnostics of a step)
-        auto& c        = d->red3;
-        const bool hit = c.valid && c.block == d->blk[d->cur] && c.epoch == d->write_epoch &&
-                         c.nin == nin && c.handles[0] == handles[0] &&
-                         (nin == RED_SCAL ||
-                          (c.handles[1] == handles[1] && c.handles[2] == handles[2]));
-        if (!hit) {
-            reduce3_kernel<256><<<(unsigned)blocks, 256, 0, st>>>(a);
-            ACB_CUDA_CHECK(cudaGetLastError());
-            d->launches++;
-            ACB_CUDA_CHECK(cudaMemcpyAsync(d->h_result, d->red_result, 3 * sizeof(double),
-                                           cudaMemcpyDeviceToHost, st));
-            ACB_CUDA_CHECK(cudaStreamSynchronize(st));
-            c.valid = true;
-            c.block = d->blk[d->cur];
-            c.epoch = d->write_epoch;
-            c.nin   = nin;
-            for (int w = 0; w < 3; ++w) {
-                c.handles[w] = w < nin ? handles[w] : -1;
-                c.vals[w]    = d->h_result[w];
-            }
+        // MAX, MIN and RMS together: one pass serves all three requests, and
+        // those of the scalar fields whose bytes it reads, while the block is
+        // unchanged (the diagnostics of a step)
+        auto& c    = d->red3;
+        auto match = [&](int e) {
+            return c.e[e].nin == nin && c.e[e].handles[0] == handles[0] &&
+                   (nin == RED_SCAL ||
+                    (c.e[e].handles[1] == handles[1] && c.e[e].handles[2] == handles[2]));
+        };
+        if (c.valid && c.block == d->blk[d->cur] && c.epoch == d->write_epoch)
+            for (int e = 0; e < c.n; ++e)
+                if (match(e)) {
+                    *result = c.e[e].vals[which];
+                    return AC_SUCCESS;
+                }
+        // the pass's inputs: the request's fields, then (single precision)
+        // the fields sharing their elements
+        int in[6], nf = 0;
+        for (int w = 0; w < nin; ++w)
+            in[nf++] = handles[w];
+        if (ACB_PAIRED) {
+            for (int w = 0; w < nin; ++w)
+                in[nf++] = acb_field(acb_array(handles[w]), 1 - acb_lane(handles[w]));
+            for (int x = 0; x < nf; ++x) // all distinct, or the request alone
+                for (int y = x + 1; y < nf; ++y)
+                    if (in[x] == in[y])
+                        nf = nin;
         }
-        *result = c.vals[which];
+        for (int w = 0; w < nf; ++w) {
+            a.f[w]  = d->blk[d->cur] + fidx(d->L, in[w], 0);
+            a.lo[w] = lo_field(d->lo[d->cur], d->L, in[w]);
+        }
+        // sets: the request, then each input as a scalar (a scalar request's
+        // own field excepted)
+        const int ns = nin == RED_SCAL ? nf : 1 + nf;
+        if (ns == 1)
+            reduce3_kernel<256><<<(unsigned)blocks, 256, 0, st>>>(a);
+        else if (nin == RED_SCAL)
+            reduce_sets_kernel<256, RED_SCAL, 2><<<(unsigned)blocks, 256, 0, st>>>(a);
+        else if (ns == 4)
+            reduce_sets_kernel<256, RED_VEC, 4><<<(unsigned)blocks, 256, 0, st>>>(a);
+        else
+            reduce_sets_kernel<256, RED_VEC, 7><<<(unsigned)blocks, 256, 0, st>>>(a);
+        ACB_CUDA_CHECK(cudaGetLastError());
+        d->launches++;
+        ACB_CUDA_CHECK(cudaMemcpyAsync(d->h_result, d->red_result, 3 * ns * sizeof(double),
+                                       cudaMemcpyDeviceToHost, st));
+        ACB_CUDA_CHECK(cudaStreamSynchronize(st));
+        // kept beside the entries of earlier passes on this block and epoch
+        if (!(c.valid && c.block == d->blk[d->cur] && c.epoch == d->write_epoch) ||
+            c.n + ns > ACB_RED_RECORD)
+            c.n = 0;
+        c.valid = true;
+        c.block = d->blk[d->cur];
+        c.epoch = d->write_epoch;
+        for (int t = 0; t < ns; ++t) {
+            auto& e        = c.e[c.n + t];
+            const bool req = t == 0;
+            e.nin          = req ? nin : RED_SCAL;
+            for (int w = 0; w < 3; ++w)
+                e.handles[w] = req ? (w < nin ? handles[w] : -1)
+                                   : (w == 0 ? in[nin == RED_SCAL ? t : t - 1] : -1);
+            for (int q = 0; q < 3; ++q)
+                e.vals[q] = d->h_result[3 * t + q];
+        }
+        *result = c.e[c.n].vals[which];
+        c.n += ns;
         return AC_SUCCESS;
     }
     reduce_kernel<256><<<(unsigned)blocks, 256, 0, st>>>(a);
@@ -1237,11 +1286,12 @@ acDeviceCreate(const int id, const AcMeshInfo config, Device* device_handle)
 #endif
     }
     d->red_max_blocks = d->num_sms * 8;
-    ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_partials, 3 * sizeof(double) * d->red_max_blocks));
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_partials,
+                              3 * ACB_RED_SETS * sizeof(double) * d->red_max_blocks));
     ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_counter, sizeof(unsigned)));
     ACB_CUDA_CHECK(cudaMemset(d->red_counter, 0, sizeof(unsigned)));
-    ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_result, 3 * sizeof(double)));
-    ACB_CUDA_CHECK(cudaMallocHost((void**)&d->h_result, 3 * sizeof(double)));
+    ACB_CUDA_CHECK(cudaMalloc((void**)&d->red_result, 3 * ACB_RED_SETS * sizeof(double)));
+    ACB_CUDA_CHECK(cudaMallocHost((void**)&d->h_result, 3 * ACB_RED_SETS * sizeof(double)));
     d->diag_max_ctas = d->num_sms * 8;
     ACB_CUDA_CHECK(cudaMalloc((void**)&d->diag_partials, 4 * sizeof(double) * d->diag_max_ctas));
     ACB_CUDA_CHECK(cudaMalloc((void**)&d->diag_counter, sizeof(unsigned)));

@@ -21,10 +21,16 @@
 
 enum { RED_SCAL = 1, RED_VEC = 3, RED_ALFVEN = 4 };
 
+// sets of one multi-set pass at most: a vector and six scalar fields
+constexpr int ACB_RED_SETS = 7;
+// entries a Device keeps of the passes on its current block (all eight fields
+// and a vector, with room to spare)
+constexpr int ACB_RED_RECORD = 16;
+
 struct ReduceArgs {
     Layout L;
-    const state_t* f[4];
-    const lo16_t* lo[4]; // mixed build: lo parts, lo_field views (else null)
+    const state_t* f[6];
+    const lo16_t* lo[6]; // mixed build: lo parts, lo_field views (else null)
     int nin;            // 1, 3 or 4
     int rtype;          // ReductionType
     int3 start, end;
@@ -266,6 +272,139 @@ reduce3_kernel(const ReduceArgs a)
             a.result[1] = bn;
             a.result[2] = bs;
             *a.counter  = 0u; // ready for the next launch on this stream
+        }
+    }
+}
+
+// MAX, MIN and the RMS sum of several sets in one pass: set 0 is one scalar
+// field (NIN = RED_SCAL, input 0) or one vector's length (NIN = RED_VEC, inputs
+// 0-2); sets 1 .. NS-1 are the scalar fields of the inputs that follow
+// (input s for a scalar request, s - 1 for a vector one): the vector's
+// components and, in the single-precision builds, the fields that share their
+// 8-byte elements, whose bytes the pass reads anyway. Every set's accumulators
+// are combined in exactly the order reduce3_kernel combines its three, so each
+// set's results equal a reduce3_kernel pass over it, bit for bit. partials
+// holds 3 * NS * gridDim.x doubles, result 3 * NS (set s at 3 s).
+template <int THREADS, int NIN, int NS>
+__global__ void __launch_bounds__(THREADS)
+reduce_sets_kernel(const ReduceArgs a)
+{
+    constexpr int NF = NIN == RED_SCAL ? NS : (NS - 1 > 3 ? NS - 1 : 3); // inputs
+    static_assert(NF <= 6, "at most six inputs");
+    const Layout& L = a.L;
+    const int lane  = threadIdx.x & 31;
+    const int wid   = threadIdx.x >> 5;
+    const long long gw  = ((long long)blockIdx.x * THREADS + threadIdx.x) >> 5;
+    const long long nw  = ((long long)gridDim.x * THREADS) >> 5;
+    const int rx        = a.end.x - a.start.x;
+    const int ry        = a.end.y - a.start.y;
+    double mx[NS], mn[NS], sm[NS];
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+        mx[t] = -INFINITY;
+        mn[t] = INFINITY;
+        sm[t] = 0.0;
+    }
+    for (long long r = gw; r < a.rows; r += nw) {
+        const int j          = a.start.y + (int)(r % ry);
+        const int k          = a.start.z + (int)(r / ry);
+        const long long base = lidx(L, a.start.x, j, k);
+        for (int i = lane; i < rx; i += 32) {
+            const long long id = base + i;
+            double v[NF];
+#pragma unroll
+            for (int w = 0; w < NF; ++w)
+                v[w] = red_load(a, w, id);
+#pragma unroll
+            for (int t = 0; t < NS; ++t) {
+                double m, q;
+                if (t == 0 && NIN == RED_VEC) {
+                    q = red_len2(v[0], v[1], v[2]);
+                    m = sqrt(q);
+                }
+                else {
+                    m = v[NIN == RED_SCAL ? t : t - 1];
+                    q = __dmul_rn(m, m);
+                }
+                mx[t] = fmax(mx[t], m);
+                mn[t] = fmin(mn[t], m);
+                sm[t] = sm[t] + q;
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < NS; ++t)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mx[t] = fmax(mx[t], __shfl_xor_sync(0xffffffffu, mx[t], o));
+            mn[t] = fmin(mn[t], __shfl_xor_sync(0xffffffffu, mn[t], o));
+            sm[t] = sm[t] + __shfl_xor_sync(0xffffffffu, sm[t], o);
+        }
+    __shared__ double wmx[NS][THREADS / 32], wmn[NS][THREADS / 32], wsm[NS][THREADS / 32];
+    __shared__ bool last;
+    if (lane == 0)
+#pragma unroll
+        for (int t = 0; t < NS; ++t) {
+            wmx[t][wid] = mx[t];
+            wmn[t][wid] = mn[t];
+            wsm[t][wid] = sm[t];
+        }
+    __syncthreads();
+    const unsigned G = gridDim.x;
+    if (threadIdx.x == 0) {
+        for (int t = 0; t < NS; ++t) {
+            double bx = wmx[t][0], bn = wmn[t][0], bs = wsm[t][0];
+            for (int w = 1; w < THREADS / 32; ++w) {
+                bx = fmax(bx, wmx[t][w]);
+                bn = fmin(bn, wmn[t][w]);
+                bs = bs + wsm[t][w];
+            }
+            a.partials[(3 * t) * G + blockIdx.x]     = bx;
+            a.partials[(3 * t + 1) * G + blockIdx.x] = bn;
+            a.partials[(3 * t + 2) * G + blockIdx.x] = bs;
+        }
+        __threadfence();
+        const unsigned done = atomicAdd(a.counter, 1u);
+        last                = (done == G - 1);
+    }
+    __syncthreads();
+    if (last) {
+        // the fixed-order fold of reduce_kernel, for each accumulator
+        __threadfence();
+        const volatile double* P = a.partials;
+        for (int t = 0; t < NS; ++t) {
+            double vx = -INFINITY, vn = INFINITY, vs = 0.0;
+            for (int b = threadIdx.x; b < (int)G; b += THREADS) {
+                vx = fmax(vx, P[(3 * t) * G + b]);
+                vn = fmin(vn, P[(3 * t + 1) * G + b]);
+                vs = vs + P[(3 * t + 2) * G + b];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                vx = fmax(vx, __shfl_xor_sync(0xffffffffu, vx, o));
+                vn = fmin(vn, __shfl_xor_sync(0xffffffffu, vn, o));
+                vs = vs + __shfl_xor_sync(0xffffffffu, vs, o);
+            }
+            if (lane == 0) {
+                wmx[t][wid] = vx;
+                wmn[t][wid] = vn;
+                wsm[t][wid] = vs;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int t = 0; t < NS; ++t) {
+                double bx = wmx[t][0], bn = wmn[t][0], bs = wsm[t][0];
+                for (int w = 1; w < THREADS / 32; ++w) {
+                    bx = fmax(bx, wmx[t][w]);
+                    bn = fmin(bn, wmn[t][w]);
+                    bs = bs + wsm[t][w];
+                }
+                a.result[3 * t]     = bx;
+                a.result[3 * t + 1] = bn;
+                a.result[3 * t + 2] = bs;
+            }
+            *a.counter = 0u; // ready for the next launch on this stream
         }
     }
 }

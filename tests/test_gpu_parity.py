@@ -688,6 +688,44 @@ def test_bounded_wait_gives_up_and_device_stays_usable():
 
 
 @pytest.mark.parametrize("flavour", FLAVOURS)
+def test_diagnostics_print_reads_each_array_once(flavour):
+    """The standalone's diagnostics print (samples/standalone/simulation.cc:250-310:
+    MAX, MIN and RMS of |u|, then of each of the eight fields): a pass serves
+    every request whose bytes it reads, so the print takes two passes in the
+    single-precision builds (u with the A components that share its elements;
+    lnrho with s) and six in FP64 (u with its components; lnrho, ax, ay, az, s).
+    Every value equals that of a pass made for its own request, bit for bit;
+    max and min equal the host values' and the sums agree within 1e-12."""
+    prec = abi.PRECISIONS[flavour]
+    dims = (20, 14, 11)
+    info = workload_info(prec, *dims)
+    fields = init.workload_fields(*dims, prec.np_dtype, seed=5, amplitude=0.05, velocity_mode=0.1)
+    host = abi.HostMesh(prec, info, [f.copy() for f in fields])
+    U = (abi.VTXBUF_UUX, abi.VTXBUF_UUY, abi.VTXBUF_UUZ)
+    kinds = (abi.RTYPE_MAX, abi.RTYPE_MIN, abi.RTYPE_RMS)
+    with new_device(flavour, info) as dev:
+        dev.load_mesh(host)
+        l0 = dev.launch_count()
+        got_u = [dev.reduce_vec_double(k, *U) for k in kinds]
+        got = {w: [dev.reduce_scal_double(k, w) for k in kinds] for w in range(8)}
+        passes = dev.launch_count() - l0
+        # each request first after a load: a pass of its own
+        alone = {}
+        for w in range(8):
+            dev.load_mesh(host)
+            alone[w] = [dev.reduce_scal_double(k, w) for k in kinds]
+        dev.load_mesh(host)
+        alone_u = [dev.reduce_vec_double(k, *U) for k in kinds]
+    assert passes == (6 if flavour == "dp" else 2), passes
+    assert got_u == alone_u
+    for w in range(8):
+        assert got[w] == alone[w], w
+        v = interior(fields[w].astype(np.float64))
+        assert got[w][0] == v.max() and got[w][1] == v.min(), w
+        assert got[w][2] == pytest.approx(float(np.sum(v * v)), rel=1e-12), w
+
+
+@pytest.mark.parametrize("flavour", FLAVOURS)
 def test_reduction_record_follows_every_write(flavour):
     """MAX, MIN and RMS of one field or of a vector's length come from one pass
     and are kept while nothing has written the device's blocks; a step, a
