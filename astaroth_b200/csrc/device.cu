@@ -109,7 +109,10 @@ struct device_s {
         bool valid;
         const void* block;
         unsigned long long epoch;
-        int n; // entries, of every pass taken on this block and epoch
+        int n;     // entries, of every pass taken on this block and epoch
+        bool wide; // the caller reduces several arrays of one state: passes
+                   // also take the fields they read anyway (set by a second
+                   // pass on one block and epoch, and kept)
         struct {
             int nin, handles[3];
             double vals[3]; // MAX, MIN, RMS sum
@@ -674,12 +677,17 @@ run_reduce(const Device d, cudaStream_t st, int rtype, int nin, const int* handl
                     *result = c.e[e].vals[which];
                     return AC_SUCCESS;
                 }
+        // a second pass on this block and epoch: from now on the passes take
+        // every field they read (the first pass of a state, all that a caller
+        // reducing one quantity makes, stays the three-in-one pass)
+        if (c.valid && c.block == d->blk[d->cur] && c.epoch == d->write_epoch && c.n > 0)
+            c.wide = true;
         // the pass's inputs: the request's fields, then (single precision)
         // the fields sharing their elements
         int in[6], nf = 0;
         for (int w = 0; w < nin; ++w)
             in[nf++] = handles[w];
-        if (ACB_PAIRED) {
+        if (ACB_PAIRED && c.wide) {
             for (int w = 0; w < nin; ++w)
                 in[nf++] = acb_field(acb_array(handles[w]), 1 - acb_lane(handles[w]));
             for (int x = 0; x < nf; ++x) // all distinct, or the request alone
@@ -693,7 +701,7 @@ run_reduce(const Device d, cudaStream_t st, int rtype, int nin, const int* handl
         }
         // sets: the request, then each input as a scalar (a scalar request's
         // own field excepted)
-        const int ns = nin == RED_SCAL ? nf : 1 + nf;
+        const int ns = !c.wide ? 1 : (nin == RED_SCAL ? nf : 1 + nf);
         if (ns == 1)
             reduce3_kernel<256><<<(unsigned)blocks, 256, 0, st>>>(a);
         else if (nin == RED_SCAL)

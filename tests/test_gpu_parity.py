@@ -690,11 +690,13 @@ def test_bounded_wait_gives_up_and_device_stays_usable():
 @pytest.mark.parametrize("flavour", FLAVOURS)
 def test_diagnostics_print_reads_each_array_once(flavour):
     """The standalone's diagnostics print (samples/standalone/simulation.cc:250-310:
-    MAX, MIN and RMS of |u|, then of each of the eight fields): a pass serves
-    every request whose bytes it reads, so the print takes two passes in the
+    MAX, MIN and RMS of |u|, then of each of the eight fields). Once a caller has
+    reduced two arrays of one state, a pass serves every request whose bytes it
+    reads, so from the second print on a print takes two passes in the
     single-precision builds (u with the A components that share its elements;
-    lnrho with s) and six in FP64 (u with its components; lnrho, ax, ay, az, s).
-    Every value equals that of a pass made for its own request, bit for bit;
+    lnrho with s) and six in FP64 (u with its components; lnrho, ax, ay, az, s);
+    the first takes five (nine in FP64). Every value equals that of a
+    three-in-one pass made for its request alone on a new Device, bit for bit;
     max and min equal the host values' and the sums agree within 1e-12."""
     prec = abi.PRECISIONS[flavour]
     dims = (20, 14, 11)
@@ -703,26 +705,33 @@ def test_diagnostics_print_reads_each_array_once(flavour):
     host = abi.HostMesh(prec, info, [f.copy() for f in fields])
     U = (abi.VTXBUF_UUX, abi.VTXBUF_UUY, abi.VTXBUF_UUZ)
     kinds = (abi.RTYPE_MAX, abi.RTYPE_MIN, abi.RTYPE_RMS)
+
+    def print_stats(dev):
+        l0 = dev.launch_count()
+        u = [dev.reduce_vec_double(k, *U) for k in kinds]
+        f = {w: [dev.reduce_scal_double(k, w) for k in kinds] for w in range(8)}
+        return u, f, dev.launch_count() - l0
+
     with new_device(flavour, info) as dev:
         dev.load_mesh(host)
-        l0 = dev.launch_count()
-        got_u = [dev.reduce_vec_double(k, *U) for k in kinds]
-        got = {w: [dev.reduce_scal_double(k, w) for k in kinds] for w in range(8)}
-        passes = dev.launch_count() - l0
-        # each request first after a load: a pass of its own
-        alone = {}
-        for w in range(8):
+        u1, f1, p1 = print_stats(dev)
+        dev.load_mesh(host)  # a new state: the record starts again
+        u2, f2, p2 = print_stats(dev)
+    assert (p1, p2) == ((9, 6) if flavour == "dp" else (5, 2)), (p1, p2)
+    alone = {}
+    for w in range(8):
+        with new_device(flavour, info) as dev:
             dev.load_mesh(host)
             alone[w] = [dev.reduce_scal_double(k, w) for k in kinds]
+    with new_device(flavour, info) as dev:
         dev.load_mesh(host)
         alone_u = [dev.reduce_vec_double(k, *U) for k in kinds]
-    assert passes == (6 if flavour == "dp" else 2), passes
-    assert got_u == alone_u
+    assert u1 == alone_u and u2 == alone_u
     for w in range(8):
-        assert got[w] == alone[w], w
+        assert f1[w] == alone[w] and f2[w] == alone[w], w
         v = interior(fields[w].astype(np.float64))
-        assert got[w][0] == v.max() and got[w][1] == v.min(), w
-        assert got[w][2] == pytest.approx(float(np.sum(v * v)), rel=1e-12), w
+        assert f2[w][0] == v.max() and f2[w][1] == v.min(), w
+        assert f2[w][2] == pytest.approx(float(np.sum(v * v)), rel=1e-12), w
 
 
 @pytest.mark.parametrize("flavour", FLAVOURS)
